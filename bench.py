@@ -1,0 +1,453 @@
+"""Benchmark: HNSW batch search QPS at recall@10 >= 0.95 on the 1M x 128 L2 workload, one B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Workload (seeded synthetic stand-in for SIFT1M, hnsw_vector_search_b200/datasets.py): 1,000,000
+base vectors x 128 (integer values in [0, 255], 1,000 anisotropic clusters), 10,000 held-out
+queries, k = 10; graph M = 16, ef_construction = 200, built and saved by the reference library
+(its parallel build) and loaded unchanged by this library. A step is one batch of the 10,000
+queries. The operating point is the smallest ef in the sweep whose recall@10 (against exact
+brute force) reaches 0.95.
+
+Arms:
+  default        this library on the GPU: the plain FP32 beam (reference-identical results) and the
+                 BF16 traversal with FP32 re-rank, each at its own smallest ef reaching recall
+                 0.95; `value` is the faster of the two at equal recall, `plain_fp32` the other.
+  --impl reference  the unmodified reference's HnswIndex::search_batch on all host cores.
+
+Under torchrun (N > 1) every rank searches its own replica (the HNSW path does not shard: replicas
+only); value = all ranks' queries / the slowest rank's time.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+CACHE = ROOT / "data_cache"
+N_BASE = 1_000_000
+N_QUERIES = 10_000
+K = 10
+M, EF_CONSTRUCTION, SEED = 16, 200, 42
+EF_SWEEP = [16, 24, 32, 48, 64, 96, 128, 192, 256, 384, 512]
+TARGET_RECALL = 0.95
+METRIC = "QPS at recall@10>=0.95, 1Mx128 L2, 1xB200: learned/BF16 vs plain GPU HNSW"
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def workload():
+    from hnsw_vector_search_b200.datasets import config_sift_like
+    CACHE.mkdir(exist_ok=True)
+    f = CACHE / "sift_like_1m.npz"
+    if f.exists():
+        z = np.load(f)
+        return z["base"], z["queries"]
+    base, queries = config_sift_like(N_BASE, N_QUERIES)
+    np.savez(f, base=base, queries=queries)
+    return base, queries
+
+
+def reference_graph(base) -> Path:
+    """The graph, built and saved by the reference (its parallel add on all host cores); part of
+    the CPU-baseline leg, cached on disk between runs."""
+    path = CACHE / f"sift_like_1m_M{M}_efc{EF_CONSTRUCTION}.vdx"
+    if path.exists():
+        return path
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as o
+    t = time.time()
+    ref = o.RefHnsw(128, 0, M, EF_CONSTRUCTION, SEED)
+    ref.add(base, threads=0)
+    tmp = path.with_suffix(".tmp.vdx")
+    ref.save(tmp)
+    tmp.rename(path)
+    log(f"reference build: {time.time() - t:.1f} s on {os.cpu_count()} threads")
+    return path
+
+
+def recall_at_10(ids, truth) -> float:
+    hits = 0
+    for a, b in zip(ids, truth):
+        hits += len(set(a[:K].tolist()) & set(b[:K].tolist()))
+    return hits / (len(truth) * K)
+
+
+class Clocks:
+    """Samples SM clocks and throttle reasons with nvidia-smi while the timed region runs."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[4:8]):
+                if flag.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def peaks() -> tuple[float, str]:
+    f = ROOT / "MEASURED_PEAKS.json"
+    if f.exists():
+        return float(json.loads(f.read_text())["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(name: str):
+    """Per-launch DRAM bytes of a kernel from the committed ncu summary, if present."""
+    f = ROOT / "profiles" / "roofline_traffic.txt"
+    if not f.exists():
+        return None
+    for line in f.read_text().splitlines():
+        parts = line.split()
+        if len(parts) >= 2 and parts[0] == name:
+            return float(parts[1])
+    return None
+
+
+def cpu_baseline(graph: Path, queries, ef: int, seconds_target: float = 15.0) -> dict:
+    """The reference's search_batch on all host cores, timed like bench/hnsw_eval.cpp:493-512
+    (one warm-up pass, median of timed passes), on a bounded sample of the queries."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as o
+    ref = o.RefHnsw.load(graph)
+    threads = os.cpu_count() or 1
+    sample = queries
+    probe = ref.time_search_batch(sample, K, ef, threads, 1)[0]
+    repeats = int(max(3, min(20, seconds_target / max(probe, 1e-3))))
+    times = ref.time_search_batch(sample, K, ef, threads, repeats)
+    med = float(np.median(times))
+    return {"value": len(sample) / med, "unit": "queries/s", "cores": threads, "kind": "reference",
+            "isa": o.Ref().isa(),
+            "sample": f"{len(sample)} queries x {repeats} passes (median), ef {ef}, k {K}, "
+                      f"{threads} threads, search_batch of the reference"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    base, queries = workload()
+    graph = reference_graph(base)
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as o
+    ref = o.RefHnsw.load(graph)
+    threads = os.cpu_count() or 1
+    sample = queries[:2000]
+    truth_file = CACHE / "sift_like_1m_truth_ref2000.npy"
+    if truth_file.exists():
+        truth = np.load(truth_file)
+    else:  # the reference's own exact search judges the reference's recall
+        bf = o.RefBruteForce(base.shape[1], 0)
+        bf.add(base)
+        truth, _, _ = bf.search_batch(sample, K, threads)
+        np.save(truth_file, truth)
+    chosen = EF_SWEEP[-1]
+    for ef in EF_SWEEP:
+        ids, _, _ = ref.search_batch(sample, K, ef, threads)
+        if recall_at_10(ids, truth) >= TARGET_RECALL:
+            chosen = ef
+            break
+    ids, _, _ = ref.search_batch(sample, K, chosen, threads)
+    rec = recall_at_10(ids, truth)
+    for _ in range(args.warmup):
+        ref.search_batch(sample, K, chosen, threads)
+    times = ref.time_search_batch(sample, K, chosen, threads, args.steps)
+    total = float(times.sum())
+    value = len(sample) * args.steps / total
+    line = {"metric": METRIC, "impl": "reference", "value": value, "unit": "queries/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000 * total / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "1M x 128 L2 sift-like, 10k queries, M16 efc200, k10",
+                       "ef": chosen, "recall_at_10": rec, "step": f"{len(sample)} queries"},
+            "cpu_baseline": {"value": value, "unit": "queries/s", "cores": threads,
+                             "kind": "reference", "sample": f"{len(sample)} queries per step"},
+            "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def ground_truth(base, queries):
+    """Exact top-10 ids. Computed once by this library's exact GPU brute force when a GPU is
+    present (bit-identical to the reference's BruteForceIndex, tests/test_gpu_bruteforce.py),
+    else by the reference on the host; cached."""
+    f = CACHE / "sift_like_1m_truth.npy"
+    if f.exists():
+        return np.load(f)
+    import hnsw_vector_search_b200 as v
+    if v.device_count() > 0:
+        bf = v.BruteForceIndex(base.shape[1], "l2")
+        bf.add(base)
+        ids, _, _ = bf.search_batch(queries, K)
+    else:
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import oracle as o
+        bf = o.RefBruteForce(base.shape[1], 0)
+        bf.add(base)
+        ids, _, _ = bf.search_batch(queries, K)
+    np.save(f, ids)
+    return ids
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="vdx")
+    ap.add_argument("--profile", action="store_true",
+                    help="one search launch per warm-up step on the cached workload (for ncu)")
+    ap.add_argument("--mode", default="fp32", choices=["fp32", "bf16", "fp8"])
+    ap.add_argument("--ef", type=int, default=32)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    rank, world, local = dist_env()
+
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        backend = "nccl"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+        pg = dist
+
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        if pg is not None:
+            pg.barrier()
+            pg.destroy_process_group()
+        return
+
+    import torch
+    import hnsw_vector_search_b200 as v
+
+    torch.cuda.set_device(local)
+    if args.profile:
+        profile(args, v, torch)
+        return
+    base, queries = workload()
+    cpu = None
+    if rank == 0:
+        graph = reference_graph(base)
+    if pg is not None:
+        pg.barrier()
+    graph = reference_graph(base)
+    truth = ground_truth(base, queries)
+
+    ix = v.HnswIndex.load(graph)
+    modes = [("fp32", {}), ("bf16", {"precision": "bf16", "rerank": 40})]
+    for _, o in modes:
+        ix.upload(local, o.get("precision", "fp32"))
+
+    # Operating points: the smallest swept ef reaching recall 0.95, per mode.
+    points = {}
+    sweep = {}
+    for name, o in modes:
+        for ef in EF_SWEEP:
+            ids, _, _ = ix.search_batch(queries, K, ef, device=local, **o)
+            rec = recall_at_10(ids, truth)
+            sweep.setdefault(name, []).append({"ef": ef, "recall": round(rec, 4)})
+            if rec >= TARGET_RECALL:
+                points[name] = (ef, rec)
+                break
+        else:
+            points[name] = (EF_SWEEP[-1], rec)
+
+    dev = torch.device("cuda", local)
+    q_dev = torch.from_numpy(queries).to(dev)
+    nq = len(queries)
+    ids_d = torch.empty((nq, K), dtype=torch.int32, device=dev)
+    d_d = torch.empty((nq, K), dtype=torch.float32, device=dev)
+    c_d = torch.empty(nq, dtype=torch.int32, device=dev)
+    work = torch.zeros(int(v.lib().vdx_work_words()), dtype=torch.int32, device=dev)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)  # > 126 MB L2
+    stream = torch.cuda.current_stream(dev)
+
+    def device_step(ef, o):
+        ix.search_batch_device(q_dev, K, ef, K, ids_d, d_d, c_d, work, stream=stream.cuda_stream,
+                               device=local, **o)
+
+    def timed(ef, o, steps, warmup):
+        for _ in range(warmup):
+            device_step(ef, o)
+        torch.cuda.synchronize()
+        if pg is not None:
+            pg.barrier()
+        torch.cuda.synchronize()
+        total = 0.0
+        for _ in range(steps):
+            flush.zero_()  # between timed steps: evict the L2 (not timed)
+            start = torch.cuda.Event(enable_timing=True)
+            end = torch.cuda.Event(enable_timing=True)
+            start.record(stream)
+            device_step(ef, o)
+            end.record(stream)
+            end.synchronize()
+            total += start.elapsed_time(end) / 1000.0
+        torch.cuda.synchronize()
+        if pg is not None:
+            t = torch.tensor([total], device=dev)
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            total = float(t.item())
+        return total
+
+    results = {}
+    with Clocks(local) as clocks:
+        for name, o in modes:
+            ef = points[name][0]
+            total = timed(ef, o, args.steps, args.warmup)
+            torch.cuda.synchronize()
+            st = work[16:16 + 2 * 10].cpu().numpy().view(np.uint64)
+            results[name] = {"ef": ef, "recall": points[name][1], "seconds": total,
+                             "qps": nq * world * args.steps / total, "stats": st.tolist()}
+    clock_summary = clocks.summary()
+
+    best = max(results, key=lambda n: results[n]["qps"])
+    r = results[best]
+    st = r["stats"]
+    algorithmic = st[4] + st[5] + st[6] + nq * 128 * 4  # links + rows + rerank rows + queries
+    per_launch_s = r["seconds"] / args.steps
+    achieved = algorithmic / per_launch_s / 1e9
+    peak, peak_kind = peaks()
+    traffic = ncu_traffic(f"search_{best}")
+
+    # End to end through the public host API: pinned host queries in, results out, per step.
+    h_q = torch.from_numpy(queries).pin_memory().numpy()
+    ef_best = r["ef"]
+    opts = dict(modes)[best]
+    ix.search_batch(h_q, K, ef_best, device=local, **opts)
+    if pg is not None:
+        pg.barrier()
+    e2e_total = 0.0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        ix.search_batch(h_q, K, ef_best, device=local, **opts)
+        e2e_total += time.perf_counter() - t0
+    if pg is not None:
+        t = torch.tensor([e2e_total], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_total = float(t.item())
+
+    if rank == 0:
+        cpu = cpu_baseline(graph, queries, results["fp32"]["ef"])
+    if pg is not None:
+        pg.barrier()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": r["qps"], "unit": "queries/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000 * r["seconds"] / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32" if best == "fp32" else "bf16+f32",
+            "data": "synthetic",
+            "config": {"workload": "1M x 128 L2 sift-like (1,000 anisotropic clusters), 10k queries, "
+                                   "k 10, graph M16 efc200 built+saved by the reference",
+                       "mode": best, "ef": r["ef"], "recall_at_10": round(r["recall"], 4),
+                       "l2": "flushed between timed steps (256 MB write); inputs also exceed L2",
+                       "parallelism": f"replicas x{world}"},
+            "plain_fp32": {"qps": results["fp32"]["qps"], "ef": results["fp32"]["ef"],
+                           "recall_at_10": round(results["fp32"]["recall"], 4)},
+            "modes": {n: {"qps": x["qps"], "ef": x["ef"], "recall_at_10": round(x["recall"], 4)}
+                      for n, x in results.items()},
+            "sweep": sweep,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "kernel": f"search_kernel ({best})",
+                         "algorithmic_bytes_per_launch": algorithmic},
+            "cpu_baseline": cpu,
+            "e2e": {"value": nq * world * args.steps / e2e_total, "unit": "queries/s",
+                    "h2d_bytes_per_step": int(queries.nbytes),
+                    "d2h_bytes_per_step": int(nq * K * 8 + nq * 4)},
+            "gpu_launches": args.steps,
+            "clocks": clock_summary,
+        }
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def profile(args, v, torch):
+    """`warmup` + 1 launches of the search kernel on the cached 1M workload, nothing else on
+    the GPU in between: the command the committed ncu summaries were captured from."""
+    base, queries = workload()
+    ix = v.HnswIndex.load(reference_graph(base))
+    o = {} if args.mode == "fp32" else {"precision": args.mode, "rerank": 40}
+    ix.upload(0, args.mode)
+    dev = torch.device("cuda", 0)
+    q = torch.from_numpy(queries).to(dev)
+    nq = len(queries)
+    ids = torch.empty((nq, K), dtype=torch.int32, device=dev)
+    d = torch.empty((nq, K), dtype=torch.float32, device=dev)
+    c = torch.empty(nq, dtype=torch.int32, device=dev)
+    work = torch.zeros(int(v.lib().vdx_work_words()), dtype=torch.int32, device=dev)
+    for _ in range(args.warmup + 1):
+        ix.search_batch_device(q, K, args.ef, K, ids, d, c, work, **o)
+    torch.cuda.synchronize()
+    st = work[16:36].cpu().numpy().view(np.uint64)
+    print(json.dumps({"profile": args.mode, "ef": args.ef, "stats": st.tolist()}))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,296 @@
+#pragma once
+
+// Device helpers shared by the search and brute-force kernels: 16-byte asynchronous copies into
+// shared memory, element loads for the three traversal precisions, and the warp distance.
+//
+// The warp distance reproduces the reference's AVX2 summation order (src/kernels_avx2.cpp:17-80
+// of the reference) bit for bit, so FP32 GPU distances equal the reference's exactly:
+//   lane L (0..31) is accumulator lane (j = L / 8, l = L % 8) and runs one FMA chain over the
+//   elements 32t + L of every full 32-element block; lanes 0..7 then continue over the
+//   remaining full 8-element blocks. The reduction is a butterfly whose partners are the
+//   reference's: xor 8 gives acc0 + acc1 (and acc2 + acc3), xor 16 gives
+//   (acc0 + acc1) + (acc2 + acc3), then xor 4, 2, 1 are the fixed horizontal tree
+//   ((v0 + v4) + (v2 + v6)) + ((v1 + v5) + (v3 + v7)). IEEE addition is commutative, so every
+//   lane ends with the same bits. The dim % 8 tail is summed by every lane in order; when it
+//   has four or more elements its first four products are rounded before being added (the
+//   reference's GCC 13.3 -O3 build vectorizes them), the others are single FMAs.
+// Every rounding here is explicit (__fmaf_rn, __fmul_rn, __fadd_rn, __fsub_rn), so no compiler
+// contraction can change a result.
+
+#include <cuda_bf16.h>
+#include <cuda_fp8.h>
+#include <cstdint>
+
+namespace vdx::dev {
+
+constexpr std::uint32_t kNoId = 0xFFFFFFFFu;
+constexpr std::uint32_t kFull = 0xFFFFFFFFu;
+
+enum : int { kFP32 = 0, kBF16 = 1, kFP8 = 2 };
+
+__device__ __forceinline__ std::uint32_t smem_addr(const void* p) {
+    return static_cast<std::uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// One 16-byte global -> shared copy, bypassing L1 (cp.async.cg). Both addresses 16-aligned.
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_addr(smem_dst)),
+                 "l"(gmem_src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+// Waits (in hardware, no spin loop) until at most N of this thread's groups are pending.
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Element e of a traversal row held in shared or global memory, as FP32. For FP8 rows the
+// per-vector scale is the last float of the row and multiplies every element.
+template <int P>
+__device__ __forceinline__ float row_elem(const unsigned char* row, std::uint32_t e, float scale) {
+    if constexpr (P == kFP32) {
+        return reinterpret_cast<const float*>(row)[e];
+    } else if constexpr (P == kBF16) {
+        return __bfloat162float(reinterpret_cast<const __nv_bfloat16*>(row)[e]);
+    } else {
+        const __nv_fp8_e4m3 v = reinterpret_cast<const __nv_fp8_e4m3*>(row)[e];
+        return __fmul_rn(scale, static_cast<float>(v));
+    }
+}
+
+template <int P>
+__device__ __forceinline__ float row_scale(const unsigned char* row, std::uint32_t row_bytes) {
+    if constexpr (P == kFP8) {
+        return *reinterpret_cast<const float*>(row + row_bytes - 4);
+    } else {
+        return 1.0F;
+    }
+}
+
+// The raw sum between the query (FP32, shared memory, `dim` floats) and one row, computed by
+// the whole warp in the reference's order; every lane returns the same value. kL2: squared L2;
+// otherwise <q, x>.
+template <int P, bool kL2>
+__device__ __forceinline__ float warp_raw(const float* q, const unsigned char* row,
+                                          std::uint32_t dim, std::uint32_t row_bytes, int lane) {
+    const float scale = row_scale<P>(row, row_bytes);
+    const std::uint32_t blocks32 = dim >> 5;
+    float acc = 0.0F;
+#pragma unroll 4
+    for (std::uint32_t t = 0; t < blocks32; ++t) {
+        const std::uint32_t e = (t << 5) + static_cast<std::uint32_t>(lane);
+        const float x = row_elem<P>(row, e, scale);
+        const float y = q[e];
+        if constexpr (kL2) {
+            const float d = __fsub_rn(y, x);
+            acc = __fmaf_rn(d, d, acc);
+        } else {
+            acc = __fmaf_rn(y, x, acc);
+        }
+    }
+    std::uint32_t i = blocks32 << 5;
+    const std::uint32_t blocks8 = (dim - i) >> 3;
+    if (lane < 8) {
+        for (std::uint32_t r = 0; r < blocks8; ++r) {
+            const std::uint32_t e = i + (r << 3) + static_cast<std::uint32_t>(lane);
+            const float x = row_elem<P>(row, e, scale);
+            const float y = q[e];
+            if constexpr (kL2) {
+                const float d = __fsub_rn(y, x);
+                acc = __fmaf_rn(d, d, acc);
+            } else {
+                acc = __fmaf_rn(y, x, acc);
+            }
+        }
+    }
+    i += blocks8 << 3;
+    acc = __fadd_rn(acc, __shfl_xor_sync(kFull, acc, 8));
+    acc = __fadd_rn(acc, __shfl_xor_sync(kFull, acc, 16));
+    acc = __fadd_rn(acc, __shfl_xor_sync(kFull, acc, 4));
+    acc = __fadd_rn(acc, __shfl_xor_sync(kFull, acc, 2));
+    acc = __fadd_rn(acc, __shfl_xor_sync(kFull, acc, 1));
+    const std::uint32_t tail = dim - i;
+    for (std::uint32_t j = 0; j < tail; ++j) {
+        const float x = row_elem<P>(row, i + j, scale);
+        const float y = q[i + j];
+        const float a = kL2 ? __fsub_rn(y, x) : y;
+        const float b = kL2 ? a : x;
+        if (tail >= 4 && j < 4) {
+            acc = __fadd_rn(acc, __fmul_rn(a, b));
+        } else {
+            acc = __fmaf_rn(a, b, acc);
+        }
+    }
+    return acc;
+}
+
+// The ranking distance: squared L2, or 1 - <q, x> (inner product and cosine).
+template <int P, bool kL2>
+__device__ __forceinline__ float warp_distance(const float* q, const unsigned char* row,
+                                               std::uint32_t dim, std::uint32_t row_bytes,
+                                               int lane) {
+    const float raw = warp_raw<P, kL2>(q, row, dim, row_bytes, lane);
+    return kL2 ? raw : __fsub_rn(1.0F, raw);
+}
+
+// The same order computed by ONE thread over a whole row (32 accumulators in registers): the
+// exact distance for brute-force re-ranking, where one thread owns one candidate.
+template <bool kL2>
+__device__ __forceinline__ float thread_distance(const float* q, const float* x,
+                                                 std::uint32_t dim) {
+    float acc[32];
+#pragma unroll
+    for (int l = 0; l < 32; ++l) {
+        acc[l] = 0.0F;
+    }
+    std::uint32_t i = 0;
+    for (; dim - i >= 32; i += 32) {
+#pragma unroll
+        for (int l = 0; l < 32; ++l) {
+            const float a = q[i + l];
+            const float b = x[i + l];
+            if constexpr (kL2) {
+                const float d = __fsub_rn(a, b);
+                acc[l] = __fmaf_rn(d, d, acc[l]);
+            } else {
+                acc[l] = __fmaf_rn(a, b, acc[l]);
+            }
+        }
+    }
+    for (; dim - i >= 8; i += 8) {
+#pragma unroll
+        for (int l = 0; l < 8; ++l) {
+            const float a = q[i + l];
+            const float b = x[i + l];
+            if constexpr (kL2) {
+                const float d = __fsub_rn(a, b);
+                acc[l] = __fmaf_rn(d, d, acc[l]);
+            } else {
+                acc[l] = __fmaf_rn(a, b, acc[l]);
+            }
+        }
+    }
+    float v[8];
+#pragma unroll
+    for (int l = 0; l < 8; ++l) {
+        v[l] = __fadd_rn(__fadd_rn(acc[l], acc[l + 8]), __fadd_rn(acc[l + 16], acc[l + 24]));
+    }
+    float s = __fadd_rn(__fadd_rn(__fadd_rn(v[0], v[4]), __fadd_rn(v[2], v[6])),
+                        __fadd_rn(__fadd_rn(v[1], v[5]), __fadd_rn(v[3], v[7])));
+    const std::uint32_t tail = dim - i;
+    for (std::uint32_t j = 0; j < tail; ++j) {
+        const float a0 = q[i + j];
+        const float b0 = x[i + j];
+        const float a = kL2 ? __fsub_rn(a0, b0) : a0;
+        const float b = kL2 ? a : b0;
+        if (tail >= 4 && j < 4) {
+            s = __fadd_rn(s, __fmul_rn(a, b));
+        } else {
+            s = __fmaf_rn(a, b, s);
+        }
+    }
+    return kL2 ? s : __fsub_rn(1.0F, s);
+}
+
+// (distance, id) order of the reference's `closer` (include/vecdex/neighbor.hpp:23-25).
+__device__ __forceinline__ bool closer(float da, std::uint32_t ia, float db, std::uint32_t ib) {
+    return da < db || (da == db && ia < ib);
+}
+
+// Entries of a sorted result list carry this bit once expanded (ids stay below 2^31).
+constexpr std::uint32_t kExpanded = 0x80000000u;
+constexpr std::uint32_t kIdMask = 0x7FFFFFFFu;
+
+// Merges up to 32 scored candidates (lane j holds candidate j when `valid`) into the sorted list
+// R[0, r) of capacity ef: R = top-ef(R + candidates), candidates equal to an entry of R dropped.
+// Returns the lowest position a candidate was written to (or INT_MAX).
+__device__ __forceinline__ int merge_round(float* rd, std::uint32_t* rid, int& r, int ef,
+                                           float my_d, std::uint32_t my_id, bool valid,
+                                           int* ap, int lane, unsigned long long& dups) {
+    // A full list admits only candidates that beat its worst entry.
+    if (valid && r >= ef) {
+        valid = closer(my_d, my_id, rd[r - 1], rid[r - 1] & kIdMask);
+    }
+    int lo = 0;
+    bool adm = false;
+    if (valid) {
+        int hi = r;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (closer(rd[mid], rid[mid] & kIdMask, my_d, my_id)) {
+                lo = mid + 1;
+            } else {
+                hi = mid;
+            }
+        }
+        adm = !(lo < r && (rid[lo] & kIdMask) == my_id);
+    }
+    const std::uint32_t dupmask = __ballot_sync(kFull, valid && !adm);
+    if (lane == 0) {
+        dups += __popc(dupmask);
+    }
+    const std::uint32_t am = __ballot_sync(kFull, adm);
+    if (am == 0) {
+        return 0x7FFFFFFF;
+    }
+    int rank = 0;
+    for (std::uint32_t m = am; m != 0; m &= m - 1) {
+        const int j = __ffs(m) - 1;
+        const float dj = __shfl_sync(kFull, my_d, j);
+        const std::uint32_t ij = __shfl_sync(kFull, my_id, j);
+        rank += (adm && closer(dj, ij, my_d, my_id)) ? 1 : 0;
+    }
+    const int na = __popc(am);
+    if (adm) {
+        ap[rank] = lo;  // admitted positions in R, in closer order (non-decreasing)
+    }
+    __syncwarp();
+    const int minpos = ap[0];
+    // Shift R[minpos, r) right by the number of admitted candidates before each entry; chunks
+    // move from the top down so no entry is overwritten before it is read.
+    for (int c = (r - 1) >> 5; c >= 0 && (c << 5) + 31 >= minpos; --c) {
+        const int i = (c << 5) + lane;
+        int np = -1;
+        float di = 0.0F;
+        std::uint32_t ii = 0;
+        if (i >= minpos && i < r) {
+            di = rd[i];
+            ii = rid[i];
+            int a = 0, b = na;
+            while (a < b) {
+                const int m = (a + b) >> 1;
+                if (ap[m] <= i) {
+                    a = m + 1;
+                } else {
+                    b = m;
+                }
+            }
+            np = i + a;
+        }
+        __syncwarp();
+        if (np >= 0 && np < ef) {
+            rd[np] = di;
+            rid[np] = ii;
+        }
+        __syncwarp();
+    }
+    const int newpos = lo + rank;
+    const bool keep = adm && newpos < ef;
+    if (keep) {
+        rd[newpos] = my_d;
+        rid[newpos] = my_id;
+    }
+    r = min(ef, r + na);
+    int low = keep ? newpos : 0x7FFFFFFF;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        low = min(low, __shfl_xor_sync(kFull, low, o));
+    }
+    __syncwarp();
+    return low;
+}
+
+}  // namespace vdx::dev

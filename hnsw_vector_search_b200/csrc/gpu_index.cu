@@ -1,0 +1,611 @@
+// The host API's GPU side: device mirrors of an index, and the search entry points of
+// HnswIndex and BruteForceIndex that run the kernels.
+//
+// Device mirrors are built on first use (and rebuilt after add()), under the index's mutex, so
+// concurrent searches share one mirror. Each host thread keeps its own stream and its own
+// device buffers for queries and results (thread_local, grown on demand), so concurrent
+// searches never share scratch state, like the reference's scratch pool
+// (src/search_scratch.hpp:61-105). Errors come back as the reference's exception types:
+// std::invalid_argument for bad queries (with its messages), std::runtime_error for CUDA
+// failures. There is no CPU search path: without a usable GPU every search throws.
+
+#include <cuda_bf16.h>
+#include <cuda_fp8.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <format>
+#include <limits>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../host/src/internal.hpp"
+#include "bruteforce.cuh"
+#include "common.cuh"
+#include "gpu_runtime.cuh"
+#include "search.cuh"
+#include "vdx/brute_force.hpp"
+#include "vdx/device.hpp"
+#include "vdx/hnsw.hpp"
+
+namespace vdx {
+
+struct DeviceBase {
+    dev::BaseView view{};
+    int device = 0;
+    void* alloc = nullptr;
+    ~DeviceBase() {
+        if (alloc != nullptr) {
+            int prev = 0;
+            cudaGetDevice(&prev);
+            cudaSetDevice(device);
+            cudaFree(alloc);
+            cudaSetDevice(prev);
+        }
+    }
+};
+
+DeviceGraph::~DeviceGraph() {
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(device);
+    for (void* p : {vectors_alloc, vectors32_alloc, links0_alloc, upper_at_alloc, links_up_alloc}) {
+        if (p != nullptr) {
+            cudaFree(p);
+        }
+    }
+    cudaSetDevice(prev);
+}
+
+namespace gpu {
+
+void check(cudaError_t err, const char* what) {
+    if (err != cudaSuccess) {
+        throw CudaError(std::format("vdx: {}: CUDA error {} ({})", what, static_cast<int>(err),
+                                    cudaGetErrorString(err)));
+    }
+}
+
+void use_device(int device) {
+    int count = 0;
+    const cudaError_t err = cudaGetDeviceCount(&count);
+    if (err != cudaSuccess || count == 0) {
+        throw CudaError("vdx: no CUDA device is available; this library searches on the GPU only");
+    }
+    if (device < 0 || device >= count) {
+        throw std::invalid_argument(std::format("vdx: device {} does not exist ({} found)", device, count));
+    }
+    check(cudaSetDevice(device), "cudaSetDevice");
+}
+
+void* device_alloc(std::size_t bytes, const char* what) {
+    void* p = nullptr;
+    check(cudaMalloc(&p, bytes == 0 ? 16 : bytes), what);
+    return p;
+}
+
+Workspace& workspace(int device) {
+    thread_local std::vector<std::unique_ptr<Workspace>> per_device;
+    if (per_device.size() <= static_cast<std::size_t>(device)) {
+        per_device.resize(device + 1);
+    }
+    auto& ws = per_device[device];
+    if (!ws) {
+        ws = std::make_unique<Workspace>();
+        ws->device = device;
+        check(cudaStreamCreateWithFlags(&ws->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        ws->small = static_cast<std::uint32_t*>(device_alloc(256, "workspace"));
+        check(cudaMallocHost(reinterpret_cast<void**>(&ws->small_host), 256), "cudaMallocHost");
+    }
+    return *ws;
+}
+
+Workspace::~Workspace() {
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(device);
+    for (void* p : {static_cast<void*>(queries), static_cast<void*>(ids), static_cast<void*>(dists),
+                    static_cast<void*>(counts), static_cast<void*>(small), scratch}) {
+        if (p != nullptr) {
+            cudaFree(p);
+        }
+    }
+    if (small_host != nullptr) {
+        cudaFreeHost(small_host);
+    }
+    if (stream != nullptr) {
+        cudaStreamDestroy(stream);
+    }
+    cudaSetDevice(prev);
+}
+
+void Workspace::reserve(std::size_t nq, std::size_t dim, std::size_t width) {
+    const auto grow = [](auto*& p, std::size_t& cap, std::size_t need, const char* what) {
+        if (need > cap) {
+            if (p != nullptr) {
+                cudaFree(p);
+                p = nullptr;
+            }
+            const std::size_t bytes = std::max<std::size_t>(need, 1) * sizeof(*p);
+            p = static_cast<std::remove_reference_t<decltype(p)>>(device_alloc(bytes, what));
+            cap = need;
+        }
+    };
+    grow(queries, queries_cap, nq * dim, "query buffer");
+    grow(ids, ids_cap, nq * width, "result ids");
+    grow(dists, dists_cap, nq * width, "result distances");
+    grow(counts, counts_cap, nq, "result counts");
+}
+
+void* Workspace::scratch_bytes(std::size_t bytes) {
+    if (bytes > scratch_cap) {
+        if (scratch != nullptr) {
+            cudaFree(scratch);
+        }
+        scratch = device_alloc(bytes, "scratch");
+        scratch_cap = bytes;
+    }
+    return scratch;
+}
+
+// Resets the status words (code 0, first bad row UINT32_MAX), the claim counter and the stats.
+void reset_small(Workspace& ws) {
+    check(cudaMemsetAsync(ws.small, 0, 256, ws.stream), "cudaMemsetAsync");
+    check(cudaMemsetAsync(ws.small + 1, 0xFF, 4, ws.stream), "cudaMemsetAsync");
+}
+
+// Throws the reference's exception for a status word set by a kernel.
+void raise_status(std::uint32_t code, const char* where) {
+    switch (code) {
+        case dev::kErrNone:
+            return;
+        case dev::kErrNonFinite:
+            throw std::invalid_argument(std::format("{}: query must not contain NaN or inf", where));
+        case dev::kErrZeroCosine:
+            throw std::invalid_argument(
+                std::format("{}: the cosine metric can't normalize a zero query", where));
+        case dev::kErrBounds:
+            throw std::runtime_error(std::format("{}: the device graph holds an out-of-range link", where));
+        case dev::kErrCapacity:
+            throw std::invalid_argument(std::format("{}: ef exceeds the GPU search capacity", where));
+        default:
+            throw std::runtime_error(std::format("{}: device error {}", where, code));
+    }
+}
+
+}  // namespace gpu
+
+namespace {
+
+std::uint32_t round_up(std::uint32_t x, std::uint32_t m) { return (x + m - 1) / m * m; }
+
+// Layer-0 blocks [count, ids...] of stride 1 + cap -> fixed blocks of `stride`, unused slots
+// 0xFFFFFFFF.
+__global__ void repack_links_kernel(const std::uint32_t* src, std::uint32_t* dst, std::uint32_t n,
+                                    std::uint32_t cap, std::uint32_t stride) {
+    const std::size_t total = static_cast<std::size_t>(n) * stride;
+    for (std::size_t x = blockIdx.x * static_cast<std::size_t>(blockDim.x) + threadIdx.x; x < total;
+         x += static_cast<std::size_t>(gridDim.x) * blockDim.x) {
+        const std::size_t node = x / stride;
+        const std::uint32_t j = static_cast<std::uint32_t>(x - node * stride);
+        const std::uint32_t* block = src + node * (1 + cap);
+        const std::uint32_t count = block[0];
+        dst[x] = (j < count && j < cap) ? block[1 + j] : dev::kNoId;
+    }
+}
+
+// FP32 rows -> BF16 rows (round to nearest even), rows of `out_row` elements, zero padded.
+__global__ void to_bf16_kernel(const float* src, std::uint32_t src_row, __nv_bfloat16* dst,
+                               std::uint32_t out_row, std::uint32_t n, std::uint32_t dim) {
+    const std::size_t total = static_cast<std::size_t>(n) * out_row;
+    for (std::size_t x = blockIdx.x * static_cast<std::size_t>(blockDim.x) + threadIdx.x; x < total;
+         x += static_cast<std::size_t>(gridDim.x) * blockDim.x) {
+        const std::size_t r = x / out_row;
+        const std::uint32_t e = static_cast<std::uint32_t>(x - r * out_row);
+        dst[x] = __float2bfloat16_rn(e < dim ? src[r * src_row + e] : 0.0F);
+    }
+}
+
+// FP32 rows -> FP8 E4M3 rows with one FP32 scale per row (max |x| / 448, stored in the row's
+// last 4 bytes); one warp per row.
+__global__ void to_fp8_kernel(const float* src, std::uint32_t src_row, unsigned char* dst,
+                              std::uint32_t row_bytes, std::uint32_t n, std::uint32_t dim) {
+    const int lane = threadIdx.x & 31;
+    const std::size_t warp = (blockIdx.x * static_cast<std::size_t>(blockDim.x) + threadIdx.x) >> 5;
+    const std::size_t warps = (static_cast<std::size_t>(gridDim.x) * blockDim.x) >> 5;
+    for (std::size_t r = warp; r < n; r += warps) {
+        const float* x = src + r * src_row;
+        float m = 0.0F;
+        for (std::uint32_t e = lane; e < dim; e += 32) {
+            m = fmaxf(m, fabsf(x[e]));
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            m = fmaxf(m, __shfl_xor_sync(0xFFFFFFFFu, m, o));
+        }
+        const float scale = m > 0.0F ? m / 448.0F : 1.0F;
+        unsigned char* row = dst + r * row_bytes;
+        for (std::uint32_t e = lane; e < row_bytes - 4; e += 32) {
+            const float v = e < dim ? x[e] / scale : 0.0F;
+            row[e] = static_cast<unsigned char>(__nv_cvt_float_to_fp8(v, __NV_SATFINITE, __NV_E4M3));
+        }
+        if (lane == 0) {
+            *reinterpret_cast<float*>(row + row_bytes - 4) = scale;
+        }
+    }
+}
+
+std::unique_ptr<DeviceGraph> upload_graph(const HnswIndex& index, int device, Precision precision) {
+    gpu::use_device(device);
+    auto dg = std::make_unique<DeviceGraph>();
+    dg->device = device;
+    const std::uint32_t n = static_cast<std::uint32_t>(index.size());
+    const std::uint32_t dim = static_cast<std::uint32_t>(index.dim());
+    const std::uint32_t M = static_cast<std::uint32_t>(index.params().M);
+    if (index.size() >= (std::size_t{1} << 31)) {
+        throw std::length_error("vdx: the GPU search holds at most 2^31 - 1 nodes");
+    }
+    if (M > 64) {
+        throw std::invalid_argument("vdx: the GPU search supports M up to 64");
+    }
+    DeviceGraphView& v = dg->view;
+    v.n = n;
+    v.dim = dim;
+    v.row32 = round_up(dim, 4);
+    v.cap0 = 2 * M;
+    v.stride0 = round_up(2 * M, 4);
+    v.cap_up = M;
+    v.stride_up = round_up(M, 4);
+    v.max_level = static_cast<std::uint32_t>(index.max_level());
+    v.entry = index.entry_point();
+    v.metric = static_cast<std::uint32_t>(index.metric());
+    v.precision = static_cast<std::uint32_t>(precision);
+    cudaStream_t stream = gpu::workspace(device).stream;
+
+    // FP32 rows, padded to 16 bytes.
+    const std::size_t bytes32 = static_cast<std::size_t>(n) * v.row32 * 4;
+    dg->vectors32_alloc = gpu::device_alloc(bytes32, "vectors");
+    dg->bytes += bytes32;
+    {
+        std::vector<float> padded;
+        const float* src = index.vectors().data();
+        if (v.row32 != dim) {
+            padded.assign(static_cast<std::size_t>(n) * v.row32, 0.0F);
+            for (std::size_t r = 0; r < n; ++r) {
+                std::memcpy(padded.data() + r * v.row32, src + r * dim, dim * 4);
+            }
+            src = padded.data();
+        }
+        gpu::check(cudaMemcpyAsync(dg->vectors32_alloc, src, bytes32, cudaMemcpyHostToDevice, stream),
+                   "upload vectors");
+        gpu::check(cudaStreamSynchronize(stream), "upload vectors");
+    }
+    v.vectors32 = static_cast<const float*>(dg->vectors32_alloc);
+    if (precision == Precision::FP32) {
+        v.vectors = v.vectors32;
+        v.row_bytes = v.row32 * 4;
+    } else if (precision == Precision::BF16) {
+        const std::uint32_t row = round_up(dim, 8);
+        v.row_bytes = row * 2;
+        const std::size_t b = static_cast<std::size_t>(n) * v.row_bytes;
+        dg->vectors_alloc = gpu::device_alloc(b, "bf16 vectors");
+        dg->bytes += b;
+        if (n > 0) {
+            to_bf16_kernel<<<1184, 256, 0, stream>>>(v.vectors32, v.row32,
+                                                     static_cast<__nv_bfloat16*>(dg->vectors_alloc), row, n, dim);
+            gpu::check(cudaGetLastError(), "bf16 conversion");
+        }
+        v.vectors = dg->vectors_alloc;
+    } else {
+        v.row_bytes = round_up(dim + 4, 16);
+        const std::size_t b = static_cast<std::size_t>(n) * v.row_bytes;
+        dg->vectors_alloc = gpu::device_alloc(b, "fp8 vectors");
+        dg->bytes += b;
+        if (n > 0) {
+            to_fp8_kernel<<<1184, 256, 0, stream>>>(v.vectors32, v.row32,
+                                                    static_cast<unsigned char*>(dg->vectors_alloc),
+                                                    v.row_bytes, n, dim);
+            gpu::check(cudaGetLastError(), "fp8 conversion");
+        }
+        v.vectors = dg->vectors_alloc;
+    }
+
+    // Layer-0 links: upload the reference layout, repack on the device.
+    {
+        const std::size_t raw_bytes = static_cast<std::size_t>(n) * (1 + v.cap0) * 4;
+        void* raw = gpu::device_alloc(raw_bytes, "raw links");
+        gpu::check(cudaMemcpyAsync(raw, index.layer0().data(), raw_bytes, cudaMemcpyHostToDevice, stream),
+                   "upload links");
+        const std::size_t b = static_cast<std::size_t>(n) * v.stride0 * 4;
+        dg->links0_alloc = gpu::device_alloc(b, "layer-0 links");
+        dg->bytes += b;
+        if (n > 0) {
+            repack_links_kernel<<<1184, 256, 0, stream>>>(static_cast<const std::uint32_t*>(raw),
+                                                          static_cast<std::uint32_t*>(dg->links0_alloc), n,
+                                                          v.cap0, v.stride0);
+            gpu::check(cudaGetLastError(), "repack links");
+        }
+        gpu::check(cudaStreamSynchronize(stream), "repack links");
+        cudaFree(raw);
+    }
+    v.links0 = static_cast<const std::uint32_t*>(dg->links0_alloc);
+
+    // Upper layers: per-node index of the first block, blocks repacked on the host (they are few).
+    {
+        std::vector<std::uint32_t> at(n, 0);
+        std::vector<std::uint32_t> blocks;
+        const auto levels = index.levels();
+        std::uint32_t next = 0;
+        for (std::uint32_t i = 0; i < n; ++i) {
+            at[i] = next;
+            const auto own = index.upper_blocks(i);
+            for (std::uint32_t l = 0; l < levels[i]; ++l) {
+                const std::uint32_t* b = own.data() + static_cast<std::size_t>(l) * (1 + M);
+                for (std::uint32_t j = 0; j < v.stride_up; ++j) {
+                    blocks.push_back(j < b[0] && j < M ? b[1 + j] : dev::kNoId);
+                }
+            }
+            next += levels[i];
+        }
+        dg->upper_at_alloc = gpu::device_alloc(at.size() * 4, "upper index");
+        dg->links_up_alloc = gpu::device_alloc(blocks.size() * 4, "upper links");
+        dg->bytes += at.size() * 4 + blocks.size() * 4;
+        gpu::check(cudaMemcpy(dg->upper_at_alloc, at.data(), at.size() * 4, cudaMemcpyHostToDevice),
+                   "upload upper index");
+        gpu::check(cudaMemcpy(dg->links_up_alloc, blocks.data(), blocks.size() * 4, cudaMemcpyHostToDevice),
+                   "upload upper links");
+    }
+    v.upper_at = static_cast<const std::uint32_t*>(dg->upper_at_alloc);
+    v.links_up = static_cast<const std::uint32_t*>(dg->links_up_alloc);
+    return dg;
+}
+
+}  // namespace
+
+const DeviceGraph& HnswIndex::device_graph(int device, Precision precision) const {
+    if (!device_mutex_) {
+        device_mutex_ = std::make_unique<std::mutex>();
+    }
+    const std::scoped_lock lock(*device_mutex_);
+    const std::size_t slot = static_cast<std::size_t>(device) * 3 + static_cast<std::size_t>(precision);
+    if (device_.size() <= slot) {
+        device_.resize(slot + 1);
+    }
+    if (!device_[slot]) {
+        device_[slot] = upload_graph(*this, device, precision);
+    }
+    return *device_[slot];
+}
+
+void HnswIndex::search_batch_into(MatrixView<float> queries, std::size_t k, std::size_t ef,
+                                  Id* ids, float* distances, std::uint32_t* counts,
+                                  const SearchOptions& options, const char* where) const {
+    detail::check_query_shape(where, {metric_, dim(), size()}, queries.dim(), k);
+    const std::size_t nq = queries.rows();
+    if (nq == 0) {
+        return;
+    }
+    if (size() == 0) {
+        std::fill(ids, ids + nq * k, dev::kNoId);
+        std::fill(distances, distances + nq * k, std::numeric_limits<float>::infinity());
+        std::fill(counts, counts + nq, 0U);
+        return;
+    }
+    if (k > std::numeric_limits<std::uint32_t>::max() || ef > std::numeric_limits<std::uint32_t>::max()) {
+        throw std::invalid_argument(std::format("{}: k and ef must fit in 32 bits", where));
+    }
+    const DeviceGraph& dg = device_graph(options.device, options.precision);
+    gpu::Workspace& ws = gpu::workspace(options.device);
+    ws.reserve(nq, dim(), k);
+    gpu::check(cudaMemcpyAsync(ws.queries, queries.data().data(), queries.data().size_bytes(),
+                               cudaMemcpyHostToDevice, ws.stream),
+               "copy queries");
+    gpu::reset_small(ws);
+    dev::SearchArgs a;
+    a.g = dg.view;
+    a.queries = ws.queries;
+    a.nq = static_cast<std::uint32_t>(nq);
+    a.qstride = static_cast<std::uint32_t>(dim());
+    a.k = static_cast<std::uint32_t>(k);
+    a.ef = static_cast<std::uint32_t>(ef);
+    a.out_stride = static_cast<std::uint32_t>(k);
+    a.out_ids = ws.ids;
+    a.out_dists = ws.dists;
+    a.out_counts = ws.counts;
+    a.status = ws.small;
+    a.claim = ws.small + 2;
+    a.stats = reinterpret_cast<unsigned long long*>(ws.small + 16);
+    a.rerank = options.precision == Precision::FP32 ? 0U
+                                                    : (options.rerank > 0 ? options.rerank
+                                                                          : static_cast<std::uint32_t>(4 * k));
+    const std::size_t ef_eff = std::min<std::size_t>(std::max(ef, k), size());
+    dev::SearchPlan plan = dev::default_plan(dg.view, static_cast<std::uint32_t>(ef_eff));
+    gpu::check(dev::launch_search(a, plan, ws.stream), "search kernel");
+    gpu::check(cudaMemcpyAsync(ws.small_host, ws.small, 256, cudaMemcpyDeviceToHost, ws.stream),
+               "copy status");
+    gpu::check(cudaMemcpyAsync(ids, ws.ids, nq * k * 4, cudaMemcpyDeviceToHost, ws.stream), "copy ids");
+    gpu::check(cudaMemcpyAsync(distances, ws.dists, nq * k * 4, cudaMemcpyDeviceToHost, ws.stream),
+               "copy distances");
+    gpu::check(cudaMemcpyAsync(counts, ws.counts, nq * 4, cudaMemcpyDeviceToHost, ws.stream), "copy counts");
+    gpu::check(cudaStreamSynchronize(ws.stream), "search");
+    std::memcpy(ws.last_stats, ws.small_host + 16, sizeof ws.last_stats);
+    gpu::raise_status(ws.small_host[0], where);
+}
+
+std::vector<std::vector<Neighbor>> HnswIndex::search_batch(MatrixView<float> queries, std::size_t k,
+                                                           std::size_t ef, std::size_t) const {
+    const std::size_t nq = queries.rows();
+    std::vector<std::vector<Neighbor>> out(nq);
+    if (nq == 0) {
+        detail::check_query_shape("HnswIndex::search_batch", {metric_, dim(), size()}, queries.dim(), k);
+        return out;
+    }
+    std::vector<Id> ids(nq * k);
+    std::vector<float> d(nq * k);
+    std::vector<std::uint32_t> c(nq);
+    search_batch_into(queries, k, ef, ids.data(), d.data(), c.data());
+    for (std::size_t q = 0; q < nq; ++q) {
+        out[q].reserve(c[q]);
+        for (std::uint32_t i = 0; i < c[q]; ++i) {
+            out[q].push_back({d[q * k + i], ids[q * k + i]});
+        }
+    }
+    return out;
+}
+
+std::vector<Neighbor> HnswIndex::search(std::span<const float> query, std::size_t k,
+                                        std::size_t ef) const {
+    detail::check_query("HnswIndex::search", {metric_, dim(), size()}, query, k);
+    if (size() == 0) {
+        return {};
+    }
+    std::vector<Id> ids(k);
+    std::vector<float> d(k);
+    std::uint32_t c = 0;
+    search_batch_into(MatrixView<float>(query, dim()), k, ef, ids.data(), d.data(), &c, {},
+                      "HnswIndex::search");
+    std::vector<Neighbor> out;
+    out.reserve(c);
+    for (std::uint32_t i = 0; i < c; ++i) {
+        out.push_back({d[i], ids[i]});
+    }
+    return out;
+}
+
+// ---------------------------------------------------------------------------------------------
+// BruteForceIndex
+
+BruteForceIndex::BruteForceIndex(std::size_t dim, Metric metric)
+    : metric_(metric), vectors_(dim), device_mutex_(std::make_unique<std::mutex>()) {}
+BruteForceIndex::~BruteForceIndex() = default;
+BruteForceIndex::BruteForceIndex(BruteForceIndex&&) noexcept = default;
+BruteForceIndex& BruteForceIndex::operator=(BruteForceIndex&&) noexcept = default;
+
+void BruteForceIndex::store(std::span<const float> values) {
+    if (!device_mutex_) {
+        device_mutex_ = std::make_unique<std::mutex>();
+    }
+    {
+        const std::scoped_lock lock(*device_mutex_);
+        device_.clear();
+    }
+    const std::size_t first = size();
+    vectors_.append(values);
+    if (metric_ == Metric::Cosine) {
+        for (std::size_t r = first; r < size(); ++r) {
+            detail::normalize(vectors_.row(r));
+        }
+    }
+}
+
+Id BruteForceIndex::add(std::span<const float> vector) {
+    detail::check_new_vectors("BruteForceIndex::add", {metric_, dim(), size()}, vector.size(), vector);
+    const auto id = static_cast<Id>(size());
+    store(vector);
+    return id;
+}
+
+void BruteForceIndex::add(const Matrix<float>& vectors) { add(MatrixView<float>(vectors)); }
+
+void BruteForceIndex::add(MatrixView<float> vectors) {
+    detail::check_new_vectors("BruteForceIndex::add", {metric_, dim(), size()}, vectors.dim(),
+                              vectors.data());
+    store(vectors.data());
+}
+
+const DeviceBase& BruteForceIndex::device_base(int device) const {
+    if (!device_mutex_) {
+        device_mutex_ = std::make_unique<std::mutex>();
+    }
+    const std::scoped_lock lock(*device_mutex_);
+    if (device_.size() <= static_cast<std::size_t>(device)) {
+        device_.resize(device + 1);
+    }
+    if (!device_[device]) {
+        gpu::use_device(device);
+        auto b = std::make_unique<DeviceBase>();
+        b->device = device;
+        const std::uint32_t n = static_cast<std::uint32_t>(size());
+        const std::uint32_t d = static_cast<std::uint32_t>(dim());
+        const std::uint32_t row = round_up(d, 4);
+        std::vector<float> padded(static_cast<std::size_t>(n) * row, 0.0F);
+        for (std::size_t r = 0; r < n; ++r) {
+            std::memcpy(padded.data() + r * row, vectors_.data().data() + r * d, d * 4);
+        }
+        b->alloc = gpu::device_alloc(padded.size() * 4, "brute-force vectors");
+        gpu::check(cudaMemcpy(b->alloc, padded.data(), padded.size() * 4, cudaMemcpyHostToDevice),
+                   "upload vectors");
+        b->view = {static_cast<const float*>(b->alloc), n, d, row, static_cast<std::uint32_t>(metric_)};
+        device_[device] = std::move(b);
+    }
+    return *device_[device];
+}
+
+void BruteForceIndex::search_batch_into(MatrixView<float> queries, std::size_t k, Id* ids,
+                                        float* distances, std::uint32_t* counts, BruteMethod method,
+                                        int device, const char* where) const {
+    detail::check_query_shape(where, {metric_, dim(), size()}, queries.dim(), k);
+    const std::size_t nq = queries.rows();
+    if (nq == 0) {
+        return;
+    }
+    if (size() == 0) {
+        std::fill(ids, ids + nq * k, dev::kNoId);
+        std::fill(distances, distances + nq * k, std::numeric_limits<float>::infinity());
+        std::fill(counts, counts + nq, 0U);
+        return;
+    }
+    const DeviceBase& b = device_base(device);
+    gpu::Workspace& ws = gpu::workspace(device);
+    ws.reserve(nq, dim(), k);
+    gpu::check(cudaMemcpyAsync(ws.queries, queries.data().data(), queries.data().size_bytes(),
+                               cudaMemcpyHostToDevice, ws.stream),
+               "copy queries");
+    gpu::reset_small(ws);
+    dev::BruteArgs a;
+    a.base = b.view;
+    a.queries = ws.queries;
+    a.nq = static_cast<std::uint32_t>(nq);
+    a.qstride = static_cast<std::uint32_t>(dim());
+    a.k = static_cast<std::uint32_t>(k);
+    a.out_stride = static_cast<std::uint32_t>(k);
+    a.out_ids = ws.ids;
+    a.out_dists = ws.dists;
+    a.out_counts = ws.counts;
+    a.status = ws.small;
+    if (method == BruteMethod::TensorCore) {
+        void* work = ws.scratch_bytes(dev::bruteforce_tc_workspace(a.nq, b.view.n, b.view.dim, a.k));
+        gpu::check(dev::launch_bruteforce_tc(a, work, ws.stream, ws.small + 8), "brute-force (tensor cores)");
+    } else {
+        gpu::check(dev::launch_bruteforce_exact(a, ws.stream), "brute-force kernel");
+    }
+    gpu::check(cudaMemcpyAsync(ws.small_host, ws.small, 256, cudaMemcpyDeviceToHost, ws.stream),
+               "copy status");
+    gpu::check(cudaMemcpyAsync(ids, ws.ids, nq * k * 4, cudaMemcpyDeviceToHost, ws.stream), "copy ids");
+    gpu::check(cudaMemcpyAsync(distances, ws.dists, nq * k * 4, cudaMemcpyDeviceToHost, ws.stream),
+               "copy distances");
+    gpu::check(cudaMemcpyAsync(counts, ws.counts, nq * 4, cudaMemcpyDeviceToHost, ws.stream), "copy counts");
+    gpu::check(cudaStreamSynchronize(ws.stream), "brute force");
+    gpu::raise_status(ws.small_host[0], where);
+}
+
+std::vector<Neighbor> BruteForceIndex::search(std::span<const float> query, std::size_t k) const {
+    detail::check_query("BruteForceIndex::search", {metric_, dim(), size()}, query, k);
+    if (size() == 0) {
+        return {};
+    }
+    std::vector<Id> ids(k);
+    std::vector<float> d(k);
+    std::uint32_t c = 0;
+    search_batch_into(MatrixView<float>(query, dim()), k, ids.data(), d.data(), &c);
+    std::vector<Neighbor> out;
+    for (std::uint32_t i = 0; i < c; ++i) {
+        out.push_back({d[i], ids[i]});
+    }
+    return out;
+}
+
+}  // namespace vdx

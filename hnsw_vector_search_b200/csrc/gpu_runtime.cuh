@@ -1,0 +1,55 @@
+#pragma once
+
+// Per-thread device workspace and CUDA error plumbing shared by the host entry points.
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+
+namespace vdx::gpu {
+
+// A failed CUDA call, or no usable device (the C ABI maps it to VDX_ERR_CUDA).
+struct CudaError : std::runtime_error {
+    explicit CudaError(const std::string& what) : std::runtime_error(what) {}
+};
+
+// One host thread's buffers on one device: its stream, query and result buffers (grown on
+// demand), 256 bytes of status / counter / statistics words and their pinned host copy.
+// Layout of `small` (u32 words): [0] error code, [1] first failing row, [2] work counter,
+// [3..7] spare, [8] uncertified count (tensor-core brute force), [16..] 64-bit statistics.
+struct Workspace {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    float* queries = nullptr;
+    std::size_t queries_cap = 0;
+    std::uint32_t* ids = nullptr;
+    std::size_t ids_cap = 0;
+    float* dists = nullptr;
+    std::size_t dists_cap = 0;
+    std::uint32_t* counts = nullptr;
+    std::size_t counts_cap = 0;
+    std::uint32_t* small = nullptr;
+    std::uint32_t* small_host = nullptr;
+    void* scratch = nullptr;
+    std::size_t scratch_cap = 0;
+    unsigned long long last_stats[16] = {};
+
+    Workspace() = default;
+    Workspace(const Workspace&) = delete;
+    Workspace& operator=(const Workspace&) = delete;
+    ~Workspace();
+    void reserve(std::size_t nq, std::size_t dim, std::size_t width);
+    void* scratch_bytes(std::size_t bytes);
+};
+
+void check(cudaError_t err, const char* what);
+void use_device(int device);
+void* device_alloc(std::size_t bytes, const char* what);
+Workspace& workspace(int device);
+void reset_small(Workspace& ws);
+void raise_status(std::uint32_t code, const char* where);
+
+}  // namespace vdx::gpu

@@ -1,0 +1,530 @@
+// HNSW search on the GPU: one warp per query, persistent blocks claiming queries from a counter.
+//
+// Per query (the reference's search_unchecked, src/hnsw.cpp:504-522):
+//   1. load the query into shared memory, reject NaN/inf, normalize under cosine
+//      (sqrt of the kernel-order <q, q>, IEEE division; src/vector_ops.cpp:14-34);
+//   2. greedy descent over layers max_level..1 (src/hnsw.cpp:416-431): all links of the current
+//      node are scored at once and the walk moves to the first strict minimum in link order,
+//      which is exactly where the reference's sequential running-minimum scan ends;
+//   3. the layer-0 beam (src/hnsw.cpp:438-482) over a sorted result list R of at most ef entries,
+//      each with an "expanded" bit: repeatedly expand the closest unexpanded entry, score its
+//      unvisited neighbors, and set R = top-ef(R + scored). This returns exactly the reference's
+//      result: admitting a batch is the same as admitting one at a time (both keep the top ef of
+//      everything scored), and the reference's candidate heap only ever matters through entries
+//      still in R (a popped candidate evicted from R ends the search at the same point where R
+//      has no unexpanded entry left).
+//   4. write the first min(k, |R|) entries, closest first (ties by smaller id).
+//
+// Memory traffic, the bound of this kernel: each expansion reads one link block (one 128-byte line
+// at M = 16) and gathers the unvisited neighbors' rows with 16-byte cp.async copies into shared
+// memory, all rows of a round in flight together; the link block of the next likely expansion
+// (the second-best unexpanded entry) is prefetched while the current one is processed.
+//
+// The visited set is a per-warp shared-memory open-addressing hash. It never reports an
+// unvisited node as visited. If its probe limit is reached it reports "unvisited" and the node is
+// scored again; the merge then drops the copy already in R (equal distance and id), so results
+// stay exact and the only cost is the extra row read (counted in kStatDuplicates).
+//
+// Every loop is bounded (the walk cannot run longer than the node count), and no kernel waits on
+// another thread or block: cp.async completion is a hardware wait.
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+
+#include "common.cuh"
+#include "search.cuh"
+
+namespace vdx::dev {
+namespace {
+
+constexpr int kProbes = 16;
+
+struct Counters {
+    unsigned long long v[kStatCount];
+};
+
+__device__ __forceinline__ void report(std::uint32_t* status, std::uint32_t code,
+                                       std::uint32_t row) {
+    atomicCAS(status, 0u, code);
+    atomicMin(status + 1, row);
+}
+
+// True if `id` was not seen before in this query's layer-0 search (inserts it). Never returns
+// false for an unseen id.
+__device__ __forceinline__ bool first_visit(std::uint32_t* table, std::uint32_t mask,
+                                            std::uint32_t id) {
+    std::uint32_t h = (id * 2654435761u) & mask;
+#pragma unroll 1
+    for (int p = 0; p < kProbes; ++p) {
+        const std::uint32_t old = atomicCAS(table + h, kNoId, id);
+        if (old == kNoId) {
+            return true;
+        }
+        if (old == id) {
+            return false;
+        }
+        h = (h + 1) & mask;
+    }
+    return true;
+}
+
+// Copies `count` rows (ids in `ids`, shared) of `row_bytes` each from `base` into `dst`
+// (shared), 16 bytes per lane per step, and commits them as one cp.async group.
+__device__ __forceinline__ void gather_rows(unsigned char* dst, const unsigned char* base,
+                                            const std::uint32_t* ids, std::uint32_t count,
+                                            std::uint32_t row_bytes, int lane) {
+    const std::uint32_t chunks = row_bytes >> 4;
+    const std::uint32_t total = count * chunks;
+    for (std::uint32_t x = static_cast<std::uint32_t>(lane); x < total; x += 32) {
+        const std::uint32_t r = x / chunks;
+        const std::uint32_t c = x - r * chunks;
+        cp_async16(dst + r * row_bytes + (c << 4),
+                   base + static_cast<std::size_t>(ids[r]) * row_bytes + (c << 4));
+    }
+    cp_async_commit();
+}
+
+// Index of the first unexpanded entry in R[from, r), or r if there is none.
+__device__ __forceinline__ int first_unexpanded(const std::uint32_t* rid, int from, int r,
+                                                int lane) {
+    for (int base = from & ~31; base < r; base += 32) {
+        const int i = base + lane;
+        const bool open = i >= from && i < r && (rid[i] & kExpanded) == 0;
+        const std::uint32_t m = __ballot_sync(kFull, open);
+        if (m != 0) {
+            return base + __ffs(m) - 1;
+        }
+    }
+    return r;
+}
+
+template <int P, bool kL2>
+__global__ void __launch_bounds__(256) search_kernel(const SearchArgs a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int lane = static_cast<int>(threadIdx.x & 31);
+    const int warp = static_cast<int>(threadIdx.x >> 5);
+    unsigned char* ws = smem + static_cast<std::size_t>(warp) * a.warp_bytes;
+    float* q = reinterpret_cast<float*>(ws);
+    float* rd = reinterpret_cast<float*>(ws + a.off_r);
+    std::uint32_t* rid = reinterpret_cast<std::uint32_t*>(ws + a.off_r + a.efcap * 4);
+    std::uint32_t* table = reinterpret_cast<std::uint32_t*>(ws + a.off_hash);
+    std::uint32_t* lbuf = reinterpret_cast<std::uint32_t*>(ws + a.off_links);
+    unsigned char* rows = ws + a.off_rows;
+    std::uint32_t* fresh = reinterpret_cast<std::uint32_t*>(ws + a.off_fresh);
+    int* ap = reinterpret_cast<int*>(ws + a.off_ap);
+
+    const DeviceGraphView& g = a.g;
+    const auto* vecs = static_cast<const unsigned char*>(g.vectors);
+    const std::uint32_t nq = a.nq_device != nullptr ? *a.nq_device : a.nq;
+    const std::uint32_t hmask = a.hash_slots - 1;
+    const int rounds_cap = static_cast<int>(a.rows_cap < 32 ? a.rows_cap : 32);
+
+    unsigned long long c_exp = 0, c_d0 = 0, c_du = 0, c_lb = 0, c_rb = 0, c_rr = 0, c_dup = 0,
+                       c_pf = 0, c_q = 0;
+
+    for (;;) {
+        std::uint32_t qi = 0;
+        if (lane == 0) {
+            qi = atomicAdd(a.claim, 1u);
+        }
+        qi = __shfl_sync(kFull, qi, 0);
+        if (qi >= nq) {
+            break;
+        }
+        const std::uint32_t k = a.k_per_q != nullptr ? a.k_per_q[qi] : a.k;
+        std::uint32_t efq = a.ef_per_q != nullptr ? a.ef_per_q[qi] : a.ef;
+        efq = efq > k ? efq : k;
+        efq = efq < g.n ? efq : g.n;  // exhaustive beyond n: same result (no eviction possible)
+        std::uint32_t* oid = a.out_ids + static_cast<std::size_t>(qi) * a.out_stride;
+        float* od = a.out_dists + static_cast<std::size_t>(qi) * a.out_stride;
+        if (efq > a.efcap) {
+            if (lane == 0) {
+                report(a.status, kErrCapacity, qi);
+                a.out_counts[qi] = 0;
+            }
+            continue;
+        }
+        const int ef = static_cast<int>(efq);
+
+        // 1. Query: load, check, normalize.
+        const float* src = a.queries + static_cast<std::size_t>(qi) * a.qstride;
+        bool bad = false;
+        for (std::uint32_t e = lane; e < g.dim; e += 32) {
+            const float v = src[e];
+            bad |= !isfinite(v);
+            q[e] = v;
+        }
+        __syncwarp();
+        if (__any_sync(kFull, bad)) {
+            if (lane == 0) {
+                report(a.status, kErrNonFinite, qi);
+                a.out_counts[qi] = 0;
+            }
+            for (std::uint32_t i = lane; i < a.out_stride; i += 32) {
+                oid[i] = kNoId;
+                od[i] = INFINITY;
+            }
+            continue;
+        }
+        if (g.metric == 2) {
+            const float raw = warp_raw<kFP32, false>(q, reinterpret_cast<const unsigned char*>(q),
+                                                     g.dim, g.row32 * 4, lane);
+            const float n = sqrtf(raw);
+            if (!(n > 0.0F) || !isfinite(n)) {
+                if (lane == 0) {
+                    report(a.status, kErrZeroCosine, qi);
+                    a.out_counts[qi] = 0;
+                }
+                for (std::uint32_t i = lane; i < a.out_stride; i += 32) {
+                    oid[i] = kNoId;
+                    od[i] = INFINITY;
+                }
+                continue;
+            }
+            __syncwarp();
+            for (std::uint32_t e = lane; e < g.dim; e += 32) {
+                q[e] = __fdiv_rn(q[e], n);
+            }
+            __syncwarp();
+        }
+        ++c_q;
+
+        // 2. Entry point and greedy descent.
+        std::uint32_t cur = g.entry;
+        if (lane == 0) {
+            fresh[0] = cur;
+        }
+        __syncwarp();
+        gather_rows(rows, vecs, fresh, 1, g.row_bytes, lane);
+        cp_async_wait<0>();
+        __syncwarp();
+        float curd = warp_distance<P, kL2>(q, rows, g.dim, g.row_bytes, lane);
+        ++c_du;
+        c_rb += g.row_bytes;
+        for (int layer = static_cast<int>(g.max_level); layer >= 1; --layer) {
+            for (std::uint32_t hop = 0; hop <= g.n; ++hop) {
+                const std::uint32_t* block =
+                    g.links_up + static_cast<std::size_t>(g.upper_at[cur] + layer - 1) * g.stride_up;
+                int f = 0;
+                for (std::uint32_t c0 = 0; c0 < g.cap_up; c0 += 32) {
+                    const std::uint32_t j = c0 + lane;
+                    std::uint32_t id = j < g.cap_up ? block[j] : kNoId;
+                    if (id != kNoId && id >= g.n) {
+                        report(a.status, kErrBounds, qi);
+                        id = kNoId;
+                    }
+                    const bool valid = id != kNoId;
+                    const std::uint32_t m = __ballot_sync(kFull, valid);
+                    if (valid) {
+                        fresh[f + __popc(m & ((1u << lane) - 1u))] = id;
+                    }
+                    f += __popc(m);
+                }
+                __syncwarp();
+                c_lb += 4ull * (1 + f);
+                float best_d = INFINITY;
+                int best_i = 0x7FFFFFFF;
+                for (int s0 = 0; s0 < f; s0 += rounds_cap) {
+                    const int cnt = min(rounds_cap, f - s0);
+                    gather_rows(rows, vecs, fresh + s0, cnt, g.row_bytes, lane);
+                    cp_async_wait<0>();
+                    __syncwarp();
+                    for (int j = 0; j < cnt; ++j) {
+                        const float d = warp_distance<P, kL2>(q, rows + j * g.row_bytes, g.dim,
+                                                              g.row_bytes, lane);
+                        if (d < best_d) {  // first strict minimum in link order
+                            best_d = d;
+                            best_i = s0 + j;
+                        }
+                    }
+                    __syncwarp();
+                }
+                c_du += f;
+                c_rb += static_cast<unsigned long long>(f) * g.row_bytes;
+                if (f > 0 && best_d < curd) {
+                    cur = fresh[best_i];
+                    curd = best_d;
+                    __syncwarp();
+                } else {
+                    break;
+                }
+            }
+        }
+
+        // 3. Layer-0 beam.
+        for (std::uint32_t i = lane; i < a.hash_slots; i += 32) {
+            table[i] = kNoId;
+        }
+        __syncwarp();
+        if (lane == 0) {
+            first_visit(table, hmask, cur);
+            rd[0] = curd;
+            rid[0] = cur;
+        }
+        __syncwarp();
+        int r = 1;
+        int scan = 0;
+        int slot = 0;
+        std::uint32_t prefetched = kNoId;
+        for (std::uint32_t step = 0; step <= g.n; ++step) {
+            const int p = first_unexpanded(rid, scan, r, lane);
+            if (p >= r) {
+                break;
+            }
+            const std::uint32_t node = rid[p] & kIdMask;
+            __syncwarp();
+            if (lane == 0) {
+                rid[p] = node | kExpanded;
+            }
+            scan = p + 1;
+            ++c_exp;
+            // The previous step's prefetch (if any) lands in this step's slot: finish it first,
+            // whether it is the block needed now or is about to be overwritten.
+            cp_async_wait<0>();
+            __syncwarp();
+            std::uint32_t* links = lbuf + slot * g.stride0;
+            if (prefetched != node) {
+                const std::uint32_t* src_links = g.links0 + static_cast<std::size_t>(node) * g.stride0;
+                for (std::uint32_t x = lane; x < (g.stride0 >> 2); x += 32) {
+                    cp_async16(links + 4 * x, src_links + 4 * x);
+                }
+                cp_async_commit();
+                cp_async_wait<0>();
+            } else {
+                ++c_pf;
+            }
+            __syncwarp();
+            // Prefetch the links of the next unexpanded entry into the other slot.
+            const int p2 = first_unexpanded(rid, p + 1, r, lane);
+            prefetched = kNoId;
+            if (p2 < r) {
+                prefetched = rid[p2] & kIdMask;
+                std::uint32_t* other = lbuf + (slot ^ 1) * g.stride0;
+                const std::uint32_t* src_links =
+                    g.links0 + static_cast<std::size_t>(prefetched) * g.stride0;
+                for (std::uint32_t x = lane; x < (g.stride0 >> 2); x += 32) {
+                    cp_async16(other + 4 * x, src_links + 4 * x);
+                }
+                cp_async_commit();
+            }
+            // Unvisited neighbors, in link order.
+            int f = 0;
+            int count = 0;
+            for (std::uint32_t c0 = 0; c0 < g.cap0; c0 += 32) {
+                const std::uint32_t j = c0 + lane;
+                std::uint32_t id = j < g.cap0 ? links[j] : kNoId;
+                if (id != kNoId && id >= g.n) {
+                    report(a.status, kErrBounds, qi);
+                    id = kNoId;
+                }
+                const bool present = id != kNoId;
+                count += __popc(__ballot_sync(kFull, present));
+                const bool isnew = present && first_visit(table, hmask, id);
+                const std::uint32_t m = __ballot_sync(kFull, isnew);
+                if (isnew) {
+                    fresh[f + __popc(m & ((1u << lane) - 1u))] = id;
+                }
+                f += __popc(m);
+            }
+            __syncwarp();
+            c_lb += 4ull * (1 + count);
+            for (int s0 = 0; s0 < f; s0 += rounds_cap) {
+                const int cnt = min(rounds_cap, f - s0);
+                gather_rows(rows, vecs, fresh + s0, cnt, g.row_bytes, lane);
+                cp_async_wait<0>();
+                __syncwarp();
+                float my_d = INFINITY;
+                for (int j = 0; j < cnt; ++j) {
+                    const float d = warp_distance<P, kL2>(q, rows + j * g.row_bytes, g.dim,
+                                                          g.row_bytes, lane);
+                    if (lane == j) {
+                        my_d = d;
+                    }
+                }
+                const bool valid = lane < cnt;
+                const std::uint32_t my_id = valid ? fresh[s0 + lane] : kNoId;
+                c_d0 += cnt;
+                c_rb += static_cast<unsigned long long>(cnt) * g.row_bytes;
+                __syncwarp();
+                const int low = merge_round(rd, rid, r, ef, my_d, my_id, valid, ap, lane, c_dup);
+                scan = min(scan, low);
+            }
+            slot ^= 1;
+        }
+        cp_async_wait<0>();  // a prefetch may still be in flight
+        __syncwarp();
+
+        // Optional exact FP32 re-rank of the best candidates (low-precision traversal).
+        if (a.rerank > 0 && P != kFP32) {
+            const int m = min(r, static_cast<int>(a.rerank));
+            for (int i = lane; i < m; i += 32) {
+                fresh[i] = rid[i] & kIdMask;
+            }
+            __syncwarp();
+            const std::uint32_t row32b = g.row32 * 4;
+            const int per_round = max(1, min(32, static_cast<int>((a.rows_cap * g.row_bytes) / row32b)));
+            int rr = 0;
+            for (int s0 = 0; s0 < m; s0 += per_round) {
+                const int cnt = min(per_round, m - s0);
+                gather_rows(rows, reinterpret_cast<const unsigned char*>(g.vectors32), fresh + s0,
+                            cnt, row32b, lane);
+                cp_async_wait<0>();
+                __syncwarp();
+                float my_d = INFINITY;
+                for (int j = 0; j < cnt; ++j) {
+                    const float d =
+                        warp_distance<kFP32, kL2>(q, rows + j * row32b, g.dim, row32b, lane);
+                    if (lane == j) {
+                        my_d = d;
+                    }
+                }
+                const bool valid = lane < cnt;
+                const std::uint32_t my_id = valid ? fresh[s0 + lane] : kNoId;
+                c_rr += static_cast<unsigned long long>(cnt) * row32b;
+                __syncwarp();
+                // Build the re-ranked list in R's storage from scratch: the candidates' ids are
+                // safe in `fresh`.
+                if (s0 == 0) {
+                    rr = 0;
+                }
+                unsigned long long unused = 0;
+                merge_round(rd, rid, rr, static_cast<int>(k), my_d, my_id, valid, ap, lane, unused);
+            }
+            r = rr;
+        }
+
+        // 4. Results.
+        const int cnt = min(r, static_cast<int>(k));
+        for (std::uint32_t i = lane; i < a.out_stride; i += 32) {
+            if (static_cast<int>(i) < cnt) {
+                oid[i] = rid[i] & kIdMask;
+                od[i] = rd[i];
+            } else {
+                oid[i] = kNoId;
+                od[i] = INFINITY;
+            }
+        }
+        if (lane == 0) {
+            a.out_counts[qi] = static_cast<std::uint32_t>(cnt);
+        }
+        __syncwarp();
+    }
+
+    if (a.stats != nullptr && lane == 0) {
+        atomicAdd(a.stats + kStatQueries, c_q);
+        atomicAdd(a.stats + kStatExpansions, c_exp);
+        atomicAdd(a.stats + kStatDist0, c_d0);
+        atomicAdd(a.stats + kStatDistUpper, c_du);
+        atomicAdd(a.stats + kStatLinkBytes, c_lb);
+        atomicAdd(a.stats + kStatRowBytes, c_rb);
+        atomicAdd(a.stats + kStatRerankBytes, c_rr);
+        atomicAdd(a.stats + kStatDuplicates, c_dup);
+        atomicAdd(a.stats + kStatPrefetchHits, c_pf);
+    }
+}
+
+std::uint32_t round_up(std::uint32_t x, std::uint32_t m) { return (x + m - 1) / m * m; }
+
+template <int P, bool kL2>
+cudaError_t launch_typed(SearchArgs& args, const SearchPlan& plan, std::size_t smem,
+                         cudaStream_t stream) {
+    auto* kernel = &search_kernel<P, kL2>;
+    cudaError_t err =
+        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (err != cudaSuccess) {
+        return err;
+    }
+    const int threads = plan.warps_per_block * 32;
+    int blocks = plan.blocks;
+    if (blocks <= 0) {
+        int device = 0;
+        cudaGetDevice(&device);
+        int sms = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        int per_sm = 0;
+        err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
+        if (err != cudaSuccess) {
+            return err;
+        }
+        blocks = sms * (per_sm > 0 ? per_sm : 1);
+    }
+    const std::uint32_t nq = args.nq;
+    const std::uint32_t needed = (nq + plan.warps_per_block - 1) / plan.warps_per_block;
+    if (args.nq_device == nullptr && static_cast<std::uint32_t>(blocks) > needed) {
+        blocks = static_cast<int>(needed > 0 ? needed : 1);
+    }
+    kernel<<<blocks, threads, smem, stream>>>(args);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+std::size_t plan_search(SearchArgs& a, const SearchPlan& plan) {
+    const DeviceGraphView& g = a.g;
+    a.efcap = plan.efcap;
+    a.hash_slots = plan.hash_slots;
+    a.rows_cap = plan.rows_cap;
+    std::uint32_t off = round_up(g.dim, 4) * 4;  // query
+    a.off_r = off;
+    off += round_up(plan.efcap * 8, 16);
+    a.off_hash = off;
+    off += plan.hash_slots * 4;
+    a.off_links = off;
+    off += 2 * g.stride0 * 4;
+    a.off_rows = off;
+    const std::uint32_t row_area = plan.rows_cap * g.row_bytes;
+    off += round_up(row_area > g.row32 * 4 ? row_area : g.row32 * 4, 16);
+    a.off_fresh = off;
+    const std::uint32_t fresh_n = g.cap0 > g.cap_up ? g.cap0 : g.cap_up;
+    const std::uint32_t fresh_need = fresh_n > a.rerank ? fresh_n : a.rerank;
+    off += round_up((fresh_need > 32 ? fresh_need : 32) * 4, 16);
+    a.off_ap = off;
+    off += 32 * 4;
+    a.off_hist = off;
+    off += 16 * 4;
+    a.warp_bytes = round_up(off, 16);
+    return static_cast<std::size_t>(a.warp_bytes) * plan.warps_per_block;
+}
+
+SearchPlan default_plan(const DeviceGraphView& g, std::uint32_t max_ef) {
+    SearchPlan p;
+    std::uint32_t cap = 32;
+    while (cap < max_ef) {
+        cap <<= 1;
+    }
+    p.efcap = cap;
+    // Measured on the 1M x 128 workload: at most ~1.5k nodes visited per query at ef = 64 and
+    // ~3k at ef = 512, so 16 slots per result entry (at least 2048) keeps the load under ~0.7.
+    std::uint32_t slots = 2048;
+    while (slots < 16 * cap && slots < 32768) {
+        slots <<= 1;
+    }
+    p.hash_slots = slots;
+    p.rows_cap = g.cap0 < 32 ? (g.cap0 > 0 ? g.cap0 : 1) : 32;
+    const std::size_t per_warp =
+        round_up(g.dim, 4) * 4 + cap * 8 + slots * 4 + 2 * g.stride0 * 4 + p.rows_cap * g.row_bytes + 1024;
+    p.warps_per_block = per_warp * 4 <= 200 * 1024 ? 4 : (per_warp * 2 <= 200 * 1024 ? 2 : 1);
+    return p;
+}
+
+cudaError_t launch_search(SearchArgs& args, const SearchPlan& plan, cudaStream_t stream) {
+    const std::size_t smem = plan_search(args, plan);
+    const bool l2 = args.g.metric == 0;
+    switch (args.g.precision) {
+        case 0:
+            return l2 ? launch_typed<kFP32, true>(args, plan, smem, stream)
+                      : launch_typed<kFP32, false>(args, plan, smem, stream);
+        case 1:
+            return l2 ? launch_typed<kBF16, true>(args, plan, smem, stream)
+                      : launch_typed<kBF16, false>(args, plan, smem, stream);
+        default:
+            return l2 ? launch_typed<kFP8, true>(args, plan, smem, stream)
+                      : launch_typed<kFP8, false>(args, plan, smem, stream);
+    }
+}
+
+int search_kernels_per_launch() { return 1; }
+
+}  // namespace vdx::dev

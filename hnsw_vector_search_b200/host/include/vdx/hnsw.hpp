@@ -1,0 +1,172 @@
+#pragma once
+
+// The HNSW index. Its public API is the reference's (include/vecdex/hnsw.hpp:63-123: constructor,
+// add, search, search_batch, inspect, memory_bytes, save, load) so that a caller switches by
+// changing the namespace; the graph it holds, and the file it saves, are the reference's too
+// (docs/FORMAT.md v1), so an index saved by the reference loads here unchanged and the other way
+// round.
+//
+// What differs is where queries run. search() and search_batch() run on a B200: a device mirror
+// of the graph (vdx/device.hpp) is uploaded on first use and refreshed after add(), and every
+// query distance, traversal step and result merge runs in hand-written sm_100a kernels. There is
+// no CPU search path. Graph construction (add) runs on the host, as in the reference, and is the
+// only place host code computes distances.
+
+#include <cstddef>
+#include <cstdint>
+#include <filesystem>
+#include <memory>
+#include <mutex>
+#include <random>
+#include <span>
+#include <string>
+#include <vector>
+
+#include "vdx/distance.hpp"
+#include "vdx/matrix.hpp"
+#include "vdx/neighbor.hpp"
+
+namespace vdx {
+
+struct DeviceGraph;  // vdx/device.hpp
+
+struct HnswParams {
+    std::size_t M = 16;                            // links per node per layer; 2M on layer 0
+    static constexpr std::size_t kMaxM = 10'000;   // the reference's limit
+    std::size_t ef_construction = 200;             // candidate list size while inserting
+    std::uint64_t seed = 42;                       // seeds the level generator
+};
+
+struct GraphReport {
+    std::vector<std::string> violations;
+    std::size_t reachable = 0;  // layer-0 nodes reachable from the entry point
+    std::size_t max_level = 0;
+    double mean_degree0 = 0.0;
+};
+
+// Element type of the vector copy the layer-0 traversal reads (SearchOptions::precision).
+enum class Precision : std::uint8_t {
+    FP32 = 0,  // the stored vectors: distances bit-identical to the reference's
+    BF16 = 1,  // bfloat16 copy, FP32 accumulation; results re-ranked in FP32
+    FP8 = 2,   // FP8 E4M3 copy with one FP32 scale per vector; re-ranked in FP32
+};
+
+// GPU search knobs beyond the reference API. The defaults give the reference's results.
+struct SearchOptions {
+    Precision precision = Precision::FP32;
+    // For BF16 / FP8: how many of the best candidates are re-scored in FP32 before the top k is
+    // taken; 0 means 4k.
+    std::uint32_t rerank = 0;
+    // Learned early termination: a small network, evaluated in the kernel every 8 expansions,
+    // stops a query's layer-0 search once it predicts the top k has converged. Needs a model
+    // (HnswIndex::set_stop_model); ef stays the hard cap.
+    bool learned_stop = false;
+    float stop_threshold = 0.5F;
+    int device = 0;
+};
+
+class HnswIndex {
+public:
+    explicit HnswIndex(std::size_t dim, Metric metric = Metric::L2, HnswParams params = {});
+    ~HnswIndex();
+    HnswIndex(HnswIndex&&) noexcept;
+    HnswIndex& operator=(HnswIndex&&) noexcept;
+    HnswIndex(const HnswIndex&) = delete;
+    HnswIndex& operator=(const HnswIndex&) = delete;
+
+    std::size_t dim() const noexcept { return vectors_.dim(); }
+    std::size_t size() const noexcept { return vectors_.rows(); }
+    Metric metric() const noexcept { return metric_; }
+    const HnswParams& params() const noexcept { return params_; }
+
+    // Graph construction on the host, the reference's algorithm (serial builds are identical to
+    // the reference's, byte for byte once saved).
+    Id add(std::span<const float> vector);
+    void add(MatrixView<float> vectors, std::size_t num_threads = 1);
+    void add(const Matrix<float>& vectors, std::size_t num_threads = 1);
+
+    // Up to k nearest neighbors, closest first, ties by smaller id; ef below k is raised to k.
+    // Runs on the GPU.
+    std::vector<Neighbor> search(std::span<const float> query, std::size_t k, std::size_t ef) const;
+
+    // search() for every row, as one GPU batch. Element i equals search(row i). num_threads is
+    // accepted for source compatibility and ignored: the batch is one launch.
+    std::vector<std::vector<Neighbor>> search_batch(MatrixView<float> queries, std::size_t k,
+                                                    std::size_t ef,
+                                                    std::size_t num_threads = 0) const;
+
+    // search_batch into caller buffers of queries.rows() * k entries (ids, distances) and
+    // queries.rows() counts; rows shorter than k are padded with id 0xFFFFFFFF and +inf.
+    // `where` names the calling API in error messages.
+    void search_batch_into(MatrixView<float> queries, std::size_t k, std::size_t ef, Id* ids,
+                           float* distances, std::uint32_t* counts,
+                           const SearchOptions& options = {},
+                           const char* where = "HnswIndex::search_batch") const;
+
+    GraphReport inspect() const;
+    std::size_t memory_bytes() const noexcept;
+
+    void save(const std::filesystem::path& path) const;
+    static HnswIndex load(const std::filesystem::path& path);
+
+    // The device mirror for `device`, uploaded (or refreshed after add()) on first use.
+    // Thread-safe; the returned reference stays valid until the next add() or destruction.
+    const DeviceGraph& device_graph(int device, Precision precision) const;
+
+    // Read-only views of the graph, in the reference's in-memory layout.
+    std::span<const std::uint8_t> levels() const noexcept { return levels_; }
+    std::span<const Id> layer0() const noexcept { return layer0_; }
+    std::span<const Id> upper_blocks(Id node) const noexcept { return upper_[node]; }
+    std::span<const float> vectors() const noexcept { return vectors_.data(); }
+    Id entry_point() const noexcept { return entry_point_; }
+    std::size_t max_level() const noexcept { return max_level_; }
+
+private:
+    struct BuildLocks;
+    enum class Locking { None, PerNode };
+
+    std::size_t max_links(std::size_t layer) const noexcept {
+        return layer == 0 ? 2 * params_.M : params_.M;
+    }
+    const Id* link_block(Id node, std::size_t layer) const noexcept;
+    Id* link_block(Id node, std::size_t layer) noexcept;
+    std::span<const Id> links(Id node, std::size_t layer) const noexcept;
+    void set_links(Id node, std::size_t layer, std::span<const Neighbor> chosen) noexcept;
+    float dist(const float* a, const float* b) const noexcept;
+    const float* vector_of(Id node) const noexcept { return vectors_.row(node).data(); }
+
+    std::size_t random_level();
+    void store(std::span<const float> vector);
+    template <Locking L>
+    void insert(Id node);
+    template <Locking L>
+    void link_back(Id node, std::size_t layer, std::span<const Neighbor> chosen);
+    std::vector<Neighbor> select_neighbors(std::vector<Neighbor> candidates, std::size_t m) const;
+    template <Locking L>
+    Neighbor build_greedy(const float* query, Neighbor entry, std::size_t layer,
+                          std::vector<Id>& copy) const;
+    template <Locking L>
+    void build_search_layer(const float* query, Neighbor entry, std::size_t ef, std::size_t layer,
+                            struct BuildScratch& scratch) const;
+    template <Locking L>
+    std::span<const Id> read_links(Id node, std::size_t layer, std::vector<Id>& copy) const;
+    void check_links(const std::filesystem::path& path) const;
+    void invalidate_device() noexcept;
+
+    Metric metric_;
+    HnswParams params_;
+    double level_multiplier_;
+    std::mt19937_64 rng_;
+    Matrix<float> vectors_;  // unit length under Cosine
+    std::vector<std::uint8_t> levels_;
+    std::vector<Id> layer0_;              // n blocks of [count, ids... (2M)]
+    std::vector<std::vector<Id>> upper_;  // per node: blocks of [count, ids... (M)], layers 1..level
+    Id entry_point_ = 0;
+    std::size_t max_level_ = 0;
+
+    std::unique_ptr<BuildLocks> build_locks_;
+    mutable std::unique_ptr<std::mutex> device_mutex_;
+    mutable std::vector<std::unique_ptr<DeviceGraph>> device_;  // per (device, precision) slot
+};
+
+}  // namespace vdx

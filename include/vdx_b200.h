@@ -1,0 +1,162 @@
+/*
+ * vdx_b200: the C ABI of the B200 batched query path for vecdex HNSW indexes.
+ *
+ * This is the drop-in boundary. Every entry point takes plain pointers and sizes, returns a
+ * vdx_status, and never lets a C++ exception cross it; the message of the last failure on the
+ * calling thread is vdx_last_error(). Each function names the reference interface it replaces
+ * (paths inside the vecdex reference project, MatiiiBL/HNSW_vector_search). Error classes map to
+ * the reference's exception types: VDX_ERR_INVALID_ARGUMENT = std::invalid_argument (with the
+ * reference's messages), VDX_ERR_LENGTH = std::length_error, VDX_ERR_IO = std::runtime_error
+ * from save/load (message starting with the path).
+ *
+ * Threading: as in the reference (include/vecdex/hnsw.hpp:58-62), searches may run
+ * concurrently from several threads, but not concurrently with vdx_index_add.
+ * Ownership: handles own all their storage (host and device); callers own every buffer they pass.
+ */
+#ifndef VDX_B200_H
+#define VDX_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VDX_API __attribute__((visibility("default")))
+
+typedef enum vdx_status {
+    VDX_OK = 0,
+    VDX_ERR_INVALID_ARGUMENT = 1, /* std::invalid_argument in the reference */
+    VDX_ERR_LENGTH = 2,           /* std::length_error */
+    VDX_ERR_IO = 3,               /* std::runtime_error from save / load */
+    VDX_ERR_CUDA = 4,             /* a CUDA call failed, or no device is present */
+    VDX_ERR_INTERNAL = 5
+} vdx_status;
+
+/* Metric codes are the file format's (docs/FORMAT.md "Header"): 0 L2, 1 inner product, 2 cosine. */
+enum { VDX_METRIC_L2 = 0, VDX_METRIC_IP = 1, VDX_METRIC_COSINE = 2 };
+/* Traversal precision of the GPU search. */
+enum { VDX_FP32 = 0, VDX_BF16 = 1, VDX_FP8 = 2 };
+/* Brute-force scoring method. */
+enum { VDX_BF_EXACT = 0, VDX_BF_TENSOR_CORE = 1 };
+
+typedef struct vdx_index vdx_index;
+typedef struct vdx_bruteforce vdx_bruteforce;
+
+typedef struct vdx_index_info {
+    uint64_t size, dim, M, ef_construction, seed, max_level, entry_point, memory_bytes;
+    uint32_t metric;
+} vdx_index_info;
+
+typedef struct vdx_graph_report {
+    uint64_t violations, reachable, max_level;
+    double mean_degree0;
+} vdx_graph_report;
+
+typedef struct vdx_search_options {
+    uint32_t precision;      /* VDX_FP32 (reference-identical results), VDX_BF16, VDX_FP8 */
+    uint32_t rerank;         /* BF16 / FP8: candidates re-scored in FP32; 0 = 4k */
+    uint32_t learned_stop;   /* nonzero: learned early termination (needs a model) */
+    float stop_threshold;    /* stop when the network's "converged" probability reaches this */
+    int32_t device;
+} vdx_search_options;
+
+/* Statistics words of a search (vdx_last_stats, vdx_search_batch_device). */
+enum {
+    VDX_STAT_QUERIES = 0, VDX_STAT_EXPANSIONS, VDX_STAT_DIST_LAYER0, VDX_STAT_DIST_UPPER,
+    VDX_STAT_LINK_BYTES, VDX_STAT_ROW_BYTES, VDX_STAT_RERANK_BYTES, VDX_STAT_DUPLICATES,
+    VDX_STAT_PREFETCH_HITS, VDX_STAT_LEARNED_STOPS, VDX_STAT_COUNT
+};
+
+VDX_API const char* vdx_last_error(void);
+VDX_API const char* vdx_version(void);
+VDX_API int vdx_device_count(void);
+
+/* --- HnswIndex lifecycle (host) ------------------------------------------------------------ */
+
+/* HnswIndex(dim, metric, {M, ef_construction, seed}): include/vecdex/hnsw.hpp:67 */
+VDX_API vdx_status vdx_index_create(uint64_t dim, uint32_t metric, uint64_t M,
+                                    uint64_t ef_construction, uint64_t seed, vdx_index** out);
+VDX_API void vdx_index_free(vdx_index* index);
+/* add(MatrixView<float>, num_threads): include/vecdex/hnsw.hpp:87 (num_threads 1 = the serial,
+ * reproducible build; 0 = one thread per hardware thread) */
+VDX_API vdx_status vdx_index_add(vdx_index* index, const float* rows, uint64_t n, uint64_t dim,
+                                 uint64_t num_threads);
+/* add(span<const float>): include/vecdex/hnsw.hpp:80 */
+VDX_API vdx_status vdx_index_add_one(vdx_index* index, const float* vector, uint64_t dim,
+                                     uint32_t* id);
+/* save(path): include/vecdex/hnsw.hpp:115 */
+VDX_API vdx_status vdx_index_save(const vdx_index* index, const char* path);
+/* load(path): include/vecdex/hnsw.hpp:123 */
+VDX_API vdx_status vdx_index_load(const char* path, vdx_index** out);
+/* size() / dim() / metric() / params() / memory_bytes(): include/vecdex/hnsw.hpp:74-77,105 */
+VDX_API vdx_status vdx_index_info_get(const vdx_index* index, vdx_index_info* out);
+/* inspect(): include/vecdex/hnsw.hpp:102; the first violation's text is copied into `first`
+ * (capacity `cap` bytes, may be NULL) */
+VDX_API vdx_status vdx_index_inspect(const vdx_index* index, vdx_graph_report* out, char* first,
+                                     uint64_t cap);
+
+/* --- HNSW search on the GPU -------------------------------------------------------------- */
+
+/* search_batch(queries, k, ef): include/vecdex/hnsw.hpp:97 (src/hnsw.cpp:490-501).
+ * Host buffers: queries nq x dim; ids, dists nq x k (rows shorter than k padded with
+ * 0xFFFFFFFF / +inf); counts nq. Synchronous. opts may be NULL (FP32, device 0). */
+VDX_API vdx_status vdx_search_batch(const vdx_index* index, const float* queries, uint64_t nq,
+                                    uint64_t dim, uint64_t k, uint64_t ef, uint32_t* ids,
+                                    float* dists, uint32_t* counts,
+                                    const vdx_search_options* opts);
+/* search(query, k, ef): include/vecdex/hnsw.hpp:93; `ids`/`dists` hold k entries. */
+VDX_API vdx_status vdx_search(const vdx_index* index, const float* query, uint64_t dim,
+                              uint64_t k, uint64_t ef, uint32_t* ids, float* dists,
+                              uint32_t* count);
+/* The statistics words (VDX_STAT_*) of this thread's last vdx_search_batch. */
+VDX_API vdx_status vdx_last_stats(uint64_t* out, uint64_t count);
+
+/* Builds (or refreshes after add) the device mirror for (device, precision) now, so that the
+ * first search does not pay for the upload. */
+VDX_API vdx_status vdx_index_upload(const vdx_index* index, int32_t device, uint32_t precision);
+
+/* Device-resident batch, asynchronous on `stream` (a cudaStream_t, or NULL for the legacy
+ * default stream): the kernel-only form of vdx_search_batch for callers whose queries and
+ * results live in device memory. Per-query k and ef come from d_k / d_ef when not NULL, else
+ * k_uniform / ef_uniform; result rows are out_stride wide. d_work is caller-owned device memory
+ * of vdx_work_words() u32 words: [0] error code (0 = ok; 1 non-finite query, 2 zero cosine
+ * query, 3 corrupt device graph, 4 ef above capacity), [1] the lowest failing row, [16..] the
+ * 64-bit statistics words. The call does not wait for the kernel. */
+VDX_API uint64_t vdx_work_words(void);
+VDX_API vdx_status vdx_search_batch_device(const vdx_index* index, const float* d_queries,
+                                           uint64_t nq, uint64_t dim, const uint32_t* d_k,
+                                           const uint32_t* d_ef, uint32_t k_uniform,
+                                           uint32_t ef_uniform, uint32_t out_stride,
+                                           uint32_t* d_ids, float* d_dists, uint32_t* d_counts,
+                                           uint32_t* d_work, const vdx_search_options* opts,
+                                           void* stream);
+
+/* --- BruteForceIndex ----------------------------------------------------------------------- */
+
+/* BruteForceIndex(dim, metric): include/vecdex/brute_force.hpp:28 */
+VDX_API vdx_status vdx_bf_create(uint64_t dim, uint32_t metric, vdx_bruteforce** out);
+VDX_API void vdx_bf_free(vdx_bruteforce* index);
+/* add(const Matrix<float>&): include/vecdex/brute_force.hpp:33 */
+VDX_API vdx_status vdx_bf_add(vdx_bruteforce* index, const float* rows, uint64_t n,
+                              uint64_t dim);
+VDX_API uint64_t vdx_bf_size(const vdx_bruteforce* index);
+/* search(query, k) for every row of `queries`: include/vecdex/brute_force.hpp:36
+ * (src/brute_force.cpp:68-84), as one GPU batch. method: VDX_BF_EXACT or VDX_BF_TENSOR_CORE. */
+VDX_API vdx_status vdx_bf_search_batch(const vdx_bruteforce* index, const float* queries,
+                                       uint64_t nq, uint64_t dim, uint64_t k, uint32_t method,
+                                       uint32_t* ids, float* dists, uint32_t* counts);
+
+/* --- Host helpers (the distance kernels' order, the file checksum) -------------------------- */
+
+/* kernels::active().l2_squared / inner_product: include/vecdex/kernels.hpp:31 */
+VDX_API float vdx_host_l2(const float* a, const float* b, uint64_t dim);
+VDX_API float vdx_host_ip(const float* a, const float* b, uint64_t dim);
+/* XXH64 (the file checksum, docs/FORMAT.md "Checksum") */
+VDX_API uint64_t vdx_xxh64(const void* data, uint64_t size, uint64_t seed);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VDX_B200_H */

@@ -1,0 +1,89 @@
+"""GPU exact brute force through the C ABI against the reference's BruteForceIndex: known
+answers, and bit-exact ids and distances for every metric."""
+
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from conftest import integer_matrix, uniform_matrix
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+METHODS = ["exact", "tensor_core"]
+
+
+def method_available(gpu, method):
+    if method == "exact":
+        return True
+    bf = gpu.BruteForceIndex(4)
+    bf.add(uniform_matrix(64, 4, 1))
+    try:
+        bf.search_batch(uniform_matrix(2, 4, 2), 2, method=method)
+        return True
+    except RuntimeError:
+        return False
+
+
+@pytest.mark.parametrize("method", METHODS)
+def test_known_answers(gpu, method):
+    if not method_available(gpu, method):
+        pytest.skip("tensor-core brute force not available")
+    line = gpu.BruteForceIndex(1)
+    line.add(np.array([[10.0], [0.0], [7.0], [3.0], [-2.0]], np.float32))
+    assert line.search([2.0], 3) == [(1.0, 3), (4.0, 1), (16.0, 4)]
+    two = gpu.BruteForceIndex(1)
+    two.add(np.array([[5.0], [1.0]], np.float32))
+    assert two.search([0.0], 10) == [(1.0, 1), (25.0, 0)]
+    ties = gpu.BruteForceIndex(1)
+    ties.add(np.array([[4.0], [-4.0], [4.0], [9.0], [-4.0]], np.float32))
+    assert ties.search([0.0], 4) == [(16.0, 0), (16.0, 1), (16.0, 2), (16.0, 4)]
+    assert ties.search([0.0], 2) == [(16.0, 0), (16.0, 1)]
+    ip = gpu.BruteForceIndex(2, "ip")
+    ip.add(np.array([[1, 0], [0, 2], [3, 3]], np.float32))
+    assert ip.search([1.0, 1.0], 3) == [(-5.0, 2), (-1.0, 1), (0.0, 0)]
+    cos = gpu.BruteForceIndex(2, "cosine")
+    cos.add(np.array([[10, 0], [0, 0.5], [-3, 0]], np.float32))
+    assert cos.search([2.0, 0.0], 3) == [(0.0, 0), (1.0, 1), (2.0, 2)]
+    assert gpu.BruteForceIndex(3).search([1.0, 2.0, 3.0], 5) == []
+
+
+def test_golden_bruteforce(gpu):
+    g = np.load(GOLDEN / "kat_results.npz")
+    bf = gpu.BruteForceIndex(16)
+    bf.add(integer_matrix(1000, 16, 1))
+    ids, d, c = bf.search_batch(integer_matrix(200, 16, 2), 10)
+    np.testing.assert_array_equal(ids, g["bf_ids"])
+    np.testing.assert_array_equal(d, g["bf_dists"])
+
+
+@pytest.mark.parametrize("metric", [0, 1, 2])
+@pytest.mark.parametrize("dim", [16, 24, 100, 128])
+def test_exact_equals_reference(gpu, orc, metric, dim):
+    base = uniform_matrix(3000, dim, 1)
+    queries = uniform_matrix(100, dim, 2)
+    ref = orc.RefBruteForce(dim, metric)
+    ref.add(base)
+    bf = gpu.BruteForceIndex(dim, metric)
+    bf.add(base)
+    for k in (1, 10, 100):
+        a = bf.search_batch(queries, k)
+        b = ref.search_batch(queries, k)
+        np.testing.assert_array_equal(a[2], b[2])
+        np.testing.assert_array_equal(a[0], b[0])
+        np.testing.assert_array_equal(a[1].view(np.uint32), b[1].view(np.uint32))
+
+
+def test_errors(gpu):
+    bf = gpu.BruteForceIndex(2)
+    bf.add(np.array([[1.0, 2.0]], np.float32))
+    with pytest.raises(ValueError, match="query has dimension 1, index has 2"):
+        bf.search([1.0], 1)
+    with pytest.raises(ValueError, match="k must be positive"):
+        bf.search([1.0, 2.0], 0)
+    with pytest.raises(ValueError, match="must not contain NaN or inf"):
+        bf.search_batch(np.array([[np.nan, 0.0]], np.float32), 1)
+    with pytest.raises(ValueError, match="NaN or inf"):
+        bf.add(np.array([[np.nan, 0.0]], np.float32))
+    assert len(bf) == 1
