@@ -18,6 +18,7 @@
 // contraction can change a result.
 
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_fp8.h>
 #include <cstdint>
 
@@ -134,6 +135,130 @@ __device__ __forceinline__ float warp_distance(const float* q, const unsigned ch
                                                int lane) {
     const float raw = warp_raw<P, kL2>(q, row, dim, row_bytes, lane);
     return kL2 ? raw : __fsub_rn(1.0F, raw);
+}
+
+// Sixteen bytes of a traversal row starting at element e, as FP32: 4 (FP32), 8 (BF16) or 16
+// (FP8) elements. `row + e * sizeof(element)` must be 16-byte aligned.
+template <int P>
+struct Vec {
+    static constexpr int kPerLoad = P == kFP32 ? 4 : (P == kBF16 ? 8 : 16);
+};
+
+template <int P>
+__device__ __forceinline__ void load16(const unsigned char* row, std::uint32_t e, float scale,
+                                       float* out) {
+    if constexpr (P == kFP32) {
+        const float4 v = *reinterpret_cast<const float4*>(row + 4 * e);
+        out[0] = v.x;
+        out[1] = v.y;
+        out[2] = v.z;
+        out[3] = v.w;
+    } else if constexpr (P == kBF16) {
+        const uint4 v = *reinterpret_cast<const uint4*>(row + 2 * e);
+        const std::uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            out[2 * i] = __uint_as_float(w[i] << 16);
+            out[2 * i + 1] = __uint_as_float(w[i] & 0xFFFF0000u);
+        }
+    } else {
+        const uint4 v = *reinterpret_cast<const uint4*>(row + e);
+        const std::uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const __half2_raw lo = __nv_cvt_fp8x2_to_halfraw2(
+                static_cast<__nv_fp8x2_storage_t>(w[i] & 0xFFFFu), __NV_E4M3);
+            const __half2_raw hi = __nv_cvt_fp8x2_to_halfraw2(
+                static_cast<__nv_fp8x2_storage_t>(w[i] >> 16), __NV_E4M3);
+            const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&lo));
+            const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&hi));
+            out[4 * i] = __fmul_rn(scale, a.x);
+            out[4 * i + 1] = __fmul_rn(scale, a.y);
+            out[4 * i + 2] = __fmul_rn(scale, b.x);
+            out[4 * i + 3] = __fmul_rn(scale, b.y);
+        }
+    }
+}
+
+template <bool kL2>
+__device__ __forceinline__ void accumulate(float& acc, float q, float x) {
+    if constexpr (kL2) {
+        const float d = __fsub_rn(q, x);
+        acc = __fmaf_rn(d, d, acc);
+    } else {
+        acc = __fmaf_rn(q, x, acc);
+    }
+}
+
+// The raw sum (squared L2, or <q, x>) between the query and one row, computed by ONE lane with
+// the reference's 32 accumulator lanes held in its registers: the same chains, tree and tail as
+// warp_raw, so the bits are the same, but no shuffles and no cross-lane dependency, so a warp
+// scores up to 32 rows at once. q (FP32) and row are 16-byte aligned (shared or global memory).
+template <int P, bool kL2>
+__device__ __forceinline__ float lane_raw(const float* q, const unsigned char* row,
+                                          std::uint32_t dim, std::uint32_t row_bytes) {
+    constexpr int E = Vec<P>::kPerLoad;
+    const float scale = row_scale<P>(row, row_bytes);
+    float acc[32];
+#pragma unroll
+    for (int l = 0; l < 32; ++l) {
+        acc[l] = 0.0F;
+    }
+    std::uint32_t i = 0;
+    for (; dim - i >= 32; i += 32) {
+#pragma unroll
+        for (int u = 0; u < 32; u += E) {
+            float x[E];
+            load16<P>(row, i + u, scale, x);
+#pragma unroll
+            for (int v = 0; v < E; v += 4) {
+                const float4 qv = *reinterpret_cast<const float4*>(q + i + u + v);
+                accumulate<kL2>(acc[u + v], qv.x, x[v]);
+                accumulate<kL2>(acc[u + v + 1], qv.y, x[v + 1]);
+                accumulate<kL2>(acc[u + v + 2], qv.z, x[v + 2]);
+                accumulate<kL2>(acc[u + v + 3], qv.w, x[v + 3]);
+            }
+        }
+    }
+    for (; dim - i >= 8; i += 8) {
+#pragma unroll
+        for (int v = 0; v < 8; ++v) {
+            accumulate<kL2>(acc[v], q[i + v], row_elem<P>(row, i + v, scale));
+        }
+    }
+    float h[8];
+#pragma unroll
+    for (int l = 0; l < 8; ++l) {
+        h[l] = __fadd_rn(__fadd_rn(acc[l], acc[l + 8]), __fadd_rn(acc[l + 16], acc[l + 24]));
+    }
+    float s = __fadd_rn(__fadd_rn(__fadd_rn(h[0], h[4]), __fadd_rn(h[2], h[6])),
+                        __fadd_rn(__fadd_rn(h[1], h[5]), __fadd_rn(h[3], h[7])));
+    const std::uint32_t tail = dim - i;
+    for (std::uint32_t j = 0; j < tail; ++j) {
+        const float x = row_elem<P>(row, i + j, scale);
+        const float y = q[i + j];
+        const float a = kL2 ? __fsub_rn(y, x) : y;
+        const float b = kL2 ? a : x;
+        if (tail >= 4 && j < 4) {
+            s = __fadd_rn(s, __fmul_rn(a, b));
+        } else {
+            s = __fmaf_rn(a, b, s);
+        }
+    }
+    return s;
+}
+
+template <int P, bool kL2>
+__device__ __forceinline__ float lane_distance(const float* q, const unsigned char* row,
+                                               std::uint32_t dim, std::uint32_t row_bytes) {
+    const float raw = lane_raw<P, kL2>(q, row, dim, row_bytes);
+    return kL2 ? raw : __fsub_rn(1.0F, raw);
+}
+
+// A shared-memory row stride for `row_bytes` rows read one row per lane with 16-byte loads:
+// an odd number of 16-byte units, so the 8 lanes of each load phase hit distinct banks.
+__host__ __device__ __forceinline__ std::uint32_t padded_row_stride(std::uint32_t row_bytes) {
+    return ((row_bytes >> 4) & 1u) ? row_bytes : row_bytes + 16;
 }
 
 // The same order computed by ONE thread over a whole row (32 accumulators in registers): the

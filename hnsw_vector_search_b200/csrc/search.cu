@@ -71,19 +71,42 @@ __device__ __forceinline__ bool first_visit(std::uint32_t* table, std::uint32_t 
 }
 
 // Copies `count` rows (ids in `ids`, shared) of `row_bytes` each from `base` into `dst`
-// (shared), 16 bytes per lane per step, and commits them as one cp.async group.
-__device__ __forceinline__ void gather_rows(unsigned char* dst, const unsigned char* base,
-                                            const std::uint32_t* ids, std::uint32_t count,
-                                            std::uint32_t row_bytes, int lane) {
+// (shared, rows `dst_stride` bytes apart), 16 bytes per lane per step, and commits them as one
+// cp.async group. `shift` is log2(row_bytes / 16) when that is a power of two up to 32 (several
+// rows per warp-wide step, no division), else -1.
+__device__ __forceinline__ void gather_rows(unsigned char* dst, std::uint32_t dst_stride,
+                                            const unsigned char* base, const std::uint32_t* ids,
+                                            std::uint32_t count, std::uint32_t row_bytes, int shift,
+                                            int lane) {
     const std::uint32_t chunks = row_bytes >> 4;
-    const std::uint32_t total = count * chunks;
-    for (std::uint32_t x = static_cast<std::uint32_t>(lane); x < total; x += 32) {
-        const std::uint32_t r = x / chunks;
-        const std::uint32_t c = x - r * chunks;
-        cp_async16(dst + r * row_bytes + (c << 4),
-                   base + static_cast<std::size_t>(ids[r]) * row_bytes + (c << 4));
+    if (shift >= 0) {
+        const std::uint32_t per_step = 32u >> shift;
+        const std::uint32_t r_in = static_cast<std::uint32_t>(lane) >> shift;
+        const std::uint32_t c = static_cast<std::uint32_t>(lane) & (chunks - 1);
+        for (std::uint32_t r0 = 0; r0 < count; r0 += per_step) {
+            const std::uint32_t r = r0 + r_in;
+            if (r < count) {
+                cp_async16(dst + r * dst_stride + (c << 4),
+                           base + static_cast<std::size_t>(ids[r]) * row_bytes + (c << 4));
+            }
+        }
+    } else {
+        for (std::uint32_t r = 0; r < count; ++r) {
+            const unsigned char* src = base + static_cast<std::size_t>(ids[r]) * row_bytes;
+            for (std::uint32_t c = static_cast<std::uint32_t>(lane); c < chunks; c += 32) {
+                cp_async16(dst + r * dst_stride + (c << 4), src + (c << 4));
+            }
+        }
     }
     cp_async_commit();
+}
+
+__device__ __forceinline__ int chunk_shift(std::uint32_t row_bytes) {
+    const std::uint32_t chunks = row_bytes >> 4;
+    if (chunks == 0 || chunks > 32 || (chunks & (chunks - 1)) != 0) {
+        return -1;
+    }
+    return __ffs(chunks) - 1;
 }
 
 // Index of the first unexpanded entry in R[from, r), or r if there is none.
@@ -120,6 +143,8 @@ __global__ void __launch_bounds__(256) search_kernel(const SearchArgs a) {
     const std::uint32_t nq = a.nq_device != nullptr ? *a.nq_device : a.nq;
     const std::uint32_t hmask = a.hash_slots - 1;
     const int rounds_cap = static_cast<int>(a.rows_cap < 32 ? a.rows_cap : 32);
+    const std::uint32_t stride_s = padded_row_stride(g.row_bytes);
+    const int shift = chunk_shift(g.row_bytes);
 
     unsigned long long c_exp = 0, c_d0 = 0, c_du = 0, c_lb = 0, c_rb = 0, c_rr = 0, c_dup = 0,
                        c_pf = 0, c_q = 0;
@@ -197,10 +222,10 @@ __global__ void __launch_bounds__(256) search_kernel(const SearchArgs a) {
             fresh[0] = cur;
         }
         __syncwarp();
-        gather_rows(rows, vecs, fresh, 1, g.row_bytes, lane);
+        gather_rows(rows, stride_s, vecs, fresh, 1, g.row_bytes, shift, lane);
         cp_async_wait<0>();
         __syncwarp();
-        float curd = warp_distance<P, kL2>(q, rows, g.dim, g.row_bytes, lane);
+        float curd = lane_distance<P, kL2>(q, rows, g.dim, g.row_bytes);
         ++c_du;
         c_rb += g.row_bytes;
         for (int layer = static_cast<int>(g.max_level); layer >= 1; --layer) {
@@ -228,16 +253,28 @@ __global__ void __launch_bounds__(256) search_kernel(const SearchArgs a) {
                 int best_i = 0x7FFFFFFF;
                 for (int s0 = 0; s0 < f; s0 += rounds_cap) {
                     const int cnt = min(rounds_cap, f - s0);
-                    gather_rows(rows, vecs, fresh + s0, cnt, g.row_bytes, lane);
+                    gather_rows(rows, stride_s, vecs, fresh + s0, cnt, g.row_bytes, shift, lane);
                     cp_async_wait<0>();
                     __syncwarp();
-                    for (int j = 0; j < cnt; ++j) {
-                        const float d = warp_distance<P, kL2>(q, rows + j * g.row_bytes, g.dim,
-                                                              g.row_bytes, lane);
-                        if (d < best_d) {  // first strict minimum in link order
-                            best_d = d;
-                            best_i = s0 + j;
+                    float d = INFINITY;
+                    int idx = 0x7FFFFFFF;
+                    if (lane < cnt) {
+                        d = lane_distance<P, kL2>(q, rows + lane * stride_s, g.dim, g.row_bytes);
+                        idx = s0 + lane;
+                    }
+                    // The first strict minimum in link order: smallest (distance, position).
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) {
+                        const float od = __shfl_xor_sync(kFull, d, o);
+                        const int oi = __shfl_xor_sync(kFull, idx, o);
+                        if (od < d || (od == d && oi < idx)) {
+                            d = od;
+                            idx = oi;
                         }
+                    }
+                    if (d < best_d) {
+                        best_d = d;
+                        best_i = idx;
                     }
                     __syncwarp();
                 }
@@ -332,18 +369,14 @@ __global__ void __launch_bounds__(256) search_kernel(const SearchArgs a) {
             c_lb += 4ull * (1 + count);
             for (int s0 = 0; s0 < f; s0 += rounds_cap) {
                 const int cnt = min(rounds_cap, f - s0);
-                gather_rows(rows, vecs, fresh + s0, cnt, g.row_bytes, lane);
+                gather_rows(rows, stride_s, vecs, fresh + s0, cnt, g.row_bytes, shift, lane);
                 cp_async_wait<0>();
                 __syncwarp();
-                float my_d = INFINITY;
-                for (int j = 0; j < cnt; ++j) {
-                    const float d = warp_distance<P, kL2>(q, rows + j * g.row_bytes, g.dim,
-                                                          g.row_bytes, lane);
-                    if (lane == j) {
-                        my_d = d;
-                    }
-                }
                 const bool valid = lane < cnt;
+                float my_d = INFINITY;
+                if (valid) {
+                    my_d = lane_distance<P, kL2>(q, rows + lane * stride_s, g.dim, g.row_bytes);
+                }
                 const std::uint32_t my_id = valid ? fresh[s0 + lane] : kNoId;
                 c_d0 += cnt;
                 c_rb += static_cast<unsigned long long>(cnt) * g.row_bytes;
@@ -364,23 +397,21 @@ __global__ void __launch_bounds__(256) search_kernel(const SearchArgs a) {
             }
             __syncwarp();
             const std::uint32_t row32b = g.row32 * 4;
-            const int per_round = max(1, min(32, static_cast<int>((a.rows_cap * g.row_bytes) / row32b)));
+            const std::uint32_t stride32 = padded_row_stride(row32b);
+            const int shift32 = chunk_shift(row32b);
+            const int per_round = max(1, min(32, static_cast<int>((a.rows_cap * stride_s) / stride32)));
             int rr = 0;
             for (int s0 = 0; s0 < m; s0 += per_round) {
                 const int cnt = min(per_round, m - s0);
-                gather_rows(rows, reinterpret_cast<const unsigned char*>(g.vectors32), fresh + s0,
-                            cnt, row32b, lane);
+                gather_rows(rows, stride32, reinterpret_cast<const unsigned char*>(g.vectors32),
+                            fresh + s0, cnt, row32b, shift32, lane);
                 cp_async_wait<0>();
                 __syncwarp();
-                float my_d = INFINITY;
-                for (int j = 0; j < cnt; ++j) {
-                    const float d =
-                        warp_distance<kFP32, kL2>(q, rows + j * row32b, g.dim, row32b, lane);
-                    if (lane == j) {
-                        my_d = d;
-                    }
-                }
                 const bool valid = lane < cnt;
+                float my_d = INFINITY;
+                if (valid) {
+                    my_d = lane_distance<kFP32, kL2>(q, rows + lane * stride32, g.dim, row32b);
+                }
                 const std::uint32_t my_id = valid ? fresh[s0 + lane] : kNoId;
                 c_rr += static_cast<unsigned long long>(cnt) * row32b;
                 __syncwarp();
@@ -474,8 +505,9 @@ std::size_t plan_search(SearchArgs& a, const SearchPlan& plan) {
     a.off_links = off;
     off += 2 * g.stride0 * 4;
     a.off_rows = off;
-    const std::uint32_t row_area = plan.rows_cap * g.row_bytes;
-    off += round_up(row_area > g.row32 * 4 ? row_area : g.row32 * 4, 16);
+    const std::uint32_t row_area = plan.rows_cap * padded_row_stride(g.row_bytes);
+    const std::uint32_t row32_area = padded_row_stride(g.row32 * 4);
+    off += round_up(row_area > row32_area ? row_area : row32_area, 16);
     a.off_fresh = off;
     const std::uint32_t fresh_n = g.cap0 > g.cap_up ? g.cap0 : g.cap_up;
     const std::uint32_t fresh_need = fresh_n > a.rerank ? fresh_n : a.rerank;
@@ -502,9 +534,11 @@ SearchPlan default_plan(const DeviceGraphView& g, std::uint32_t max_ef) {
         slots <<= 1;
     }
     p.hash_slots = slots;
-    p.rows_cap = g.cap0 < 32 ? (g.cap0 > 0 ? g.cap0 : 1) : 32;
-    const std::size_t per_warp =
-        round_up(g.dim, 4) * 4 + cap * 8 + slots * 4 + 2 * g.stride0 * 4 + p.rows_cap * g.row_bytes + 1024;
+    // Rows staged per round: 16 keeps the per-warp footprint small enough for 12+ resident
+    // warps per SM with FP32 rows; expansions with more unvisited neighbors take two rounds.
+    p.rows_cap = g.cap0 < 16 ? (g.cap0 > 0 ? g.cap0 : 1) : 16;
+    const std::size_t per_warp = round_up(g.dim, 4) * 4 + cap * 8 + slots * 4 + 2 * g.stride0 * 4 +
+                                 p.rows_cap * padded_row_stride(g.row_bytes) + 1024;
     p.warps_per_block = per_warp * 4 <= 200 * 1024 ? 4 : (per_warp * 2 <= 200 * 1024 ? 2 : 1);
     return p;
 }
