@@ -12,17 +12,9 @@
 
 #include "../../include/vdx_b200.h"
 #include "../host/src/internal.hpp"
+#include "capi_internal.hpp"
 #include "gpu_runtime.cuh"
 #include "search.cuh"
-#include "vdx/brute_force.hpp"
-#include "vdx/hnsw.hpp"
-
-struct vdx_index {
-    vdx::HnswIndex index;
-};
-struct vdx_bruteforce {
-    vdx::BruteForceIndex index;
-};
 
 namespace {
 
@@ -84,6 +76,10 @@ void require(const T* p, const char* what) {
 }
 
 }  // namespace
+
+namespace vdx::capi {
+void set_last_error(const std::string& message) { g_error = message; }
+}  // namespace vdx::capi
 
 extern "C" {
 

@@ -380,6 +380,15 @@ const DeviceGraph& HnswIndex::device_graph(int device, Precision precision) cons
     return *device_[slot];
 }
 
+const DeviceGraph* HnswIndex::uploaded_graph(int device, Precision precision) const {
+    if (!device_mutex_ || device < 0) {
+        return nullptr;
+    }
+    const std::scoped_lock lock(*device_mutex_);
+    const std::size_t slot = static_cast<std::size_t>(device) * 3 + static_cast<std::size_t>(precision);
+    return slot < device_.size() ? device_[slot].get() : nullptr;
+}
+
 void HnswIndex::search_batch_into(MatrixView<float> queries, std::size_t k, std::size_t ef,
                                   Id* ids, float* distances, std::uint32_t* counts,
                                   const SearchOptions& options, const char* where) const {

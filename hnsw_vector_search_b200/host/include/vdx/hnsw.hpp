@@ -112,6 +112,9 @@ public:
     // The device mirror for `device`, uploaded (or refreshed after add()) on first use.
     // Thread-safe; the returned reference stays valid until the next add() or destruction.
     const DeviceGraph& device_graph(int device, Precision precision) const;
+    // The device mirror for `device` if it is already uploaded and current, else nullptr.
+    // Never uploads, so it never allocates.
+    const DeviceGraph* uploaded_graph(int device, Precision precision) const;
 
     // Read-only views of the graph, in the reference's in-memory layout.
     std::span<const std::uint8_t> levels() const noexcept { return levels_; }

@@ -132,6 +132,25 @@ VDX_API vdx_status vdx_search_batch_device(const vdx_index* index, const float* 
                                            uint32_t* d_work, const vdx_search_options* opts,
                                            void* stream);
 
+/* vdx_search_batch_device without d_work, for callers that cannot allocate device memory (a
+ * process whose HBM is handed out by an external pool manager, a real-time path that must not
+ * call cudaMalloc, a plugin limited to the buffers its host passes in). No counterpart in the
+ * reference, which has no device memory at all. Allocates nothing: the launch's work words live
+ * in a 256-byte file-scope device array that every GPU loading this library holds until exit
+ * (a launch needing more is rejected with VDX_ERR_LENGTH). The index must already have a
+ * device copy for (opts->device, opts->precision): call vdx_index_upload first, which does
+ * allocate. The first call on each device looks up the array's device address, so make it
+ * before any stream capture. All calls share the array and clear it before their launch;
+ * calls whose kernels overlap on the GPU race on it, so serialize them. Synchronous: returns
+ * after the batch finished, with the reference's error for a bad query row. */
+VDX_API vdx_status vdx_search_batch_device_noalloc(const vdx_index* index, const float* d_queries,
+                                                   uint64_t nq, uint64_t dim, const uint32_t* d_k,
+                                                   const uint32_t* d_ef, uint32_t k_uniform,
+                                                   uint32_t ef_uniform, uint32_t out_stride,
+                                                   uint32_t* d_ids, float* d_dists,
+                                                   uint32_t* d_counts,
+                                                   const vdx_search_options* opts, void* stream);
+
 /* --- BruteForceIndex ----------------------------------------------------------------------- */
 
 /* BruteForceIndex(dim, metric): include/vecdex/brute_force.hpp:28 */
