@@ -40,14 +40,21 @@ struct BruteArgs {
 cudaError_t launch_bruteforce_exact(const BruteArgs& args, cudaStream_t stream);
 
 // Exact top-k through the tensor cores: a tcgen05 split-BF16 GEMM scores every pair, a fused
-// epilogue keeps each query's best candidates per tile, a merge keeps the best `candidates`
+// epilogue keeps each query's best candidates per chunk, a merge keeps the best candidates
 // overall, their distances are recomputed exactly (reference order), and a query is certified
-// only if no excluded vector can beat its k-th exact distance under the GEMM's error bound;
-// uncertified queries are recomputed by launch_bruteforce_exact. `workspace` must hold
-// bruteforce_tc_workspace() bytes.
+// only if no excluded vector can beat its k-th exact distance under the scoring error bound;
+// uncertified queries are recomputed by launch_bruteforce_exact. Shapes the path does not cover
+// (k > 48, dim > 256, k > n) go to launch_bruteforce_exact directly.
+//
+// TcBase: the stored vectors prepared once (bf16 hi / lo, norms, flags, TMA descriptors).
+struct TcBase;
+cudaError_t prepare_tc_base(const BaseView& base, cudaStream_t stream, TcBase** out);
+void free_tc_base(TcBase* base);
+// `workspace` must hold bruteforce_tc_workspace() bytes; *uncertified_out (device) receives the
+// number of queries recomputed exactly. A device wait that times out sets status code 5.
 std::size_t bruteforce_tc_workspace(std::uint32_t nq, std::uint32_t n, std::uint32_t dim,
                                     std::uint32_t k);
-cudaError_t launch_bruteforce_tc(const BruteArgs& args, void* workspace, cudaStream_t stream,
-                                 std::uint32_t* uncertified_out);
+cudaError_t launch_bruteforce_tc(const BruteArgs& args, const TcBase& base, void* workspace,
+                                 cudaStream_t stream, std::uint32_t* uncertified_out);
 
 }  // namespace vdx::dev

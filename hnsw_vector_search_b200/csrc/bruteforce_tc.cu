@@ -1,14 +1,962 @@
-// Tensor-core brute force: not built yet in this revision.
+// Exact brute force through the tensor cores (tcgen05 + TMEM + TMA), certified against the
+// reference's FP32 results.
+//
+// 1. prep: each vector is split into bfloat16 hi = bf16(x) and lo = bf16(x - hi) (zero-padded to
+//    a multiple of 64 components); squared norms in FP32. For integer data in [-256, 256] (the
+//    SIFT-like workloads) lo is zero and every product and partial sum is exact in FP32.
+// 2. score (bf_tc_kernel): a CTA owns 128 queries (the MMA's M) and streams a chunk of the
+//    stored vectors through shared memory in tiles of 128 rows (N), K in 64-element swizzled
+//    chunks. One thread issues TMA loads (no multicast), one thread issues
+//    tcgen05.mma.kind::f16 (BF16 x BF16 -> FP32 in TMEM, the terms hi*hi + hi*lo + lo*hi when
+//    the data needs them), and four warps read the 128 x 128 FP32 tile out of TMEM (double
+//    buffered, so the next tile's MMAs overlap), turn scores into distances
+//    (||q||^2 + ||x||^2 - 2 q.x, or 1 - q.x) and keep each query's best `kc` candidates of the
+//    chunk in shared memory (one query per thread).
+// 3. merge (bf_tc_merge_kernel): per query, the best `kc` candidates over all chunks are
+//    re-scored with the reference's exact FP32 order (lane_distance) and sorted by `closer`.
+//    The query is certified when its k-th exact distance is below every excluded vector's
+//    lowest possible exact distance (the smallest excluded approximate distance minus the
+//    scoring error bound); for integer data the bound is exact arithmetic.
+// 4. queries that are not certified are recomputed by the exact CUDA-core kernel.
+// So the result is the reference's, ids and distance bits, for every query.
+//
+// Every mbarrier wait is bounded (1 s of %globaltimer); a timeout sets an error word, every role
+// stops, outstanding copies and MMAs are waited for (again bounded), TMEM is freed, and the host
+// raises an error. Nothing waits on another CTA.
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstring>
+#include <mutex>
+
 #include "bruteforce.cuh"
+#include "common.cuh"
 
 namespace vdx::dev {
+namespace {
 
-std::size_t bruteforce_tc_workspace(std::uint32_t, std::uint32_t, std::uint32_t, std::uint32_t) {
-    return 16;
+constexpr int kBM = 128;                        // queries per tile (MMA M, TMEM lanes)
+constexpr int kBN = 128;                        // stored rows per tile (MMA N, TMEM columns)
+constexpr int kBK = 64;                         // K elements per 128-byte swizzled chunk
+constexpr std::uint32_t kChunk = kBM * kBK * 2;  // 16 KB: one 128 x 64 bf16 chunk
+constexpr int kThreads = 256;
+constexpr std::uint64_t kWaitNs = 1000000000ull;
+constexpr std::uint32_t kTmemCols = 2 * kBN;   // two accumulator buffers
+
+// -------------------------------------------------------------------------------------------
+// PTX wrappers
+
+__device__ __forceinline__ std::uint64_t now_ns() {
+    std::uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ void mbar_init(std::uint32_t a, std::uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(a), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(std::uint32_t a, std::uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(a), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(std::uint32_t a) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(a) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(std::uint32_t a, std::uint32_t parity) {
+    std::uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(a), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Waits for the phase with `parity` to complete; false after kWaitNs or once another role has
+// aborted.
+__device__ __forceinline__ bool mbar_wait(std::uint32_t a, std::uint32_t parity,
+                                          volatile std::uint32_t* abort_flag) {
+    if (mbar_try(a, parity)) {
+        return true;
+    }
+    const std::uint64_t t0 = now_ns();
+    for (;;) {
+        if (mbar_try(a, parity)) {
+            return true;
+        }
+        if (*abort_flag != 0 || now_ns() - t0 > kWaitNs) {
+            return false;
+        }
+    }
+}
+__device__ __forceinline__ void tma_load_2d(std::uint32_t dst, const CUtensorMap* map, int x,
+                                            int y, std::uint32_t mbar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes "
+        "[%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+        "l"(reinterpret_cast<std::uint64_t>(map)), "r"(x), "r"(y), "r"(mbar)
+        : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+// Shared-memory matrix descriptor of a K-major tile written by TMA with 128-byte swizzling:
+// rows of 128 bytes, 8-row atoms 1024 bytes apart (SBO), version 1, layout SWIZZLE_128B.
+__device__ __forceinline__ std::uint64_t sw128_desc(std::uint32_t saddr) {
+    return static_cast<std::uint64_t>((saddr & 0x3FFFFu) >> 4) | (std::uint64_t{1} << 16) |
+           (std::uint64_t{1024 >> 4} << 32) | (std::uint64_t{1} << 46) | (std::uint64_t{2} << 61);
+}
+// Instruction descriptor: BF16 A and B, FP32 accumulator, both K-major, M = 128, N = 128.
+constexpr std::uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) |
+                                 (static_cast<std::uint32_t>(kBN >> 3) << 17) |
+                                 (static_cast<std::uint32_t>(kBM >> 4) << 24);
+__device__ __forceinline__ void mma_bf16(std::uint32_t d_tmem, std::uint64_t a, std::uint64_t b,
+                                         std::uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+        "l"(a), "l"(b), "r"(kIdesc), "r"(accumulate)
+        : "memory");
+}
+__device__ __forceinline__ void mma_commit(std::uint32_t mbar) {
+    asm volatile(
+        "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
+        : "memory");
+}
+__device__ __forceinline__ void tmem_ld32(std::uint32_t taddr, std::uint32_t (&r)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+          "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),
+          "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+          "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
+          "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-cudaError_t launch_bruteforce_tc(const BruteArgs&, void*, cudaStream_t, std::uint32_t*) {
-    return cudaErrorNotSupported;
+// -------------------------------------------------------------------------------------------
+// Kernel parameters
+
+struct TcParams {
+    std::uint32_t nq, n, dim, kchunks, qtiles, nchunks, chunk_rows, kc, stages, metric;
+    std::uint32_t base_lo;                // the stored vectors have nonzero lo parts
+    const std::uint32_t* query_flags;     // bit 0: some query has a nonzero lo part
+    const float* qnorm;                   // [nq]
+    const float* xnorm;                   // [n]
+    std::uint32_t* cand_ids;              // [nq][nchunks][kc]
+    float* cand_d;
+    float* cand_tau;                      // [nq][nchunks]
+    std::uint32_t* error;                 // status word: 5 on a timeout
+    std::uint32_t off_b, off_lists, off_bar;  // smem offsets from the 1024-aligned base
+};
+
+__global__ void __launch_bounds__(kThreads, 1)
+    bf_tc_kernel(const __grid_constant__ CUtensorMap tq_hi, const __grid_constant__ CUtensorMap tq_lo,
+                 const __grid_constant__ CUtensorMap tx_hi, const __grid_constant__ CUtensorMap tx_lo,
+                 const TcParams p) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    const std::uint32_t raw_addr = smem_addr(smem_raw);
+    const std::uint32_t base_addr = (raw_addr + 1023u) & ~1023u;
+    unsigned char* base = smem_raw + (base_addr - raw_addr);
+    const int warp = static_cast<int>(threadIdx.x >> 5);
+    const int lane = static_cast<int>(threadIdx.x & 31);
+
+    const std::uint32_t S = p.stages;
+    const bool qlo = (*p.query_flags & 1u) != 0;
+    const bool xlo = p.base_lo != 0;
+    const std::uint32_t a_hi = base_addr;
+    const std::uint32_t a_lo = base_addr + p.kchunks * kChunk;
+    const std::uint32_t stage_bytes = (xlo ? 2u : 1u) * p.kchunks * kChunk;
+    const std::uint32_t b0 = base_addr + p.off_b;
+    float* list_d = reinterpret_cast<float*>(base + p.off_lists);          // [kc][128]
+    std::uint32_t* list_i = reinterpret_cast<std::uint32_t*>(base + p.off_lists + p.kc * kBM * 4);
+    const std::uint32_t bar = base_addr + p.off_bar;
+    const auto full = [&](std::uint32_t s) { return bar + 8 * s; };
+    const auto empty = [&](std::uint32_t s) { return bar + 8 * (S + s); };
+    const std::uint32_t a_full = bar + 8 * (2 * S);
+    const std::uint32_t a_empty = a_full + 8;
+    const std::uint32_t tfull0 = a_full + 16;   // two
+    const std::uint32_t tempty0 = a_full + 32;  // two
+    const std::uint32_t drain = a_full + 48;
+    std::uint32_t* holder = reinterpret_cast<std::uint32_t*>(base + p.off_bar + 8 * (2 * S) + 56);
+    volatile std::uint32_t* abort_flag = holder + 1;
+
+    if (threadIdx.x == 0) {
+        for (std::uint32_t s = 0; s < S; ++s) {
+            mbar_init(full(s), 1);
+            mbar_init(empty(s), 1);
+        }
+        mbar_init(a_full, 1);
+        mbar_init(a_empty, 1);
+        mbar_init(tfull0, 1);
+        mbar_init(tfull0 + 8, 1);
+        mbar_init(tempty0, kBM);
+        mbar_init(tempty0 + 8, kBM);
+        mbar_init(drain, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_addr(holder)),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const std::uint32_t tmem = *holder;
+
+    const std::uint32_t items = p.qtiles * p.nchunks;
+    const auto fail = [&]() {
+        *abort_flag = 1;
+        atomicCAS(p.error, 0u, 5u);  // the host raises "device wait timed out"
+    };
+
+    if (warp == 0 && lane == 0) {
+        // TMA producer.
+        std::uint32_t it = 0, item_idx = 0;
+        std::uint32_t last_full[8];
+        std::uint32_t last_parity[8];
+        std::uint32_t outstanding = 0;
+        bool ok = true;
+        for (std::uint32_t item = blockIdx.x; ok && item < items; item += gridDim.x, ++item_idx) {
+            const std::uint32_t qt = item % p.qtiles;
+            const std::uint32_t ch = item / p.qtiles;
+            if (item_idx > 0 && !mbar_wait(a_empty, (item_idx - 1) & 1u, abort_flag)) {
+                fail();
+                ok = false;
+                break;
+            }
+            mbar_expect_tx(a_full, (qlo ? 2u : 1u) * p.kchunks * kChunk);
+            for (std::uint32_t c = 0; c < p.kchunks; ++c) {
+                tma_load_2d(a_hi + c * kChunk, &tq_hi, static_cast<int>(c * kBK),
+                            static_cast<int>(qt * kBM), a_full);
+                if (qlo) {
+                    tma_load_2d(a_lo + c * kChunk, &tq_lo, static_cast<int>(c * kBK),
+                                static_cast<int>(qt * kBM), a_full);
+                }
+            }
+            const std::uint32_t row0 = ch * p.chunk_rows;
+            const std::uint32_t rows = min(p.chunk_rows, p.n - row0);
+            const std::uint32_t tiles = (rows + kBN - 1) / kBN;
+            for (std::uint32_t t = 0; t < tiles; ++t, ++it) {
+                const std::uint32_t s = it % S;
+                const std::uint32_t ph = (it / S) & 1u;
+                if (!mbar_wait(empty(s), ph ^ 1u, abort_flag)) {
+                    fail();
+                    ok = false;
+                    break;
+                }
+                mbar_expect_tx(full(s), stage_bytes);
+                const std::uint32_t bs = b0 + s * stage_bytes;
+                const int y = static_cast<int>(row0 + t * kBN);
+                for (std::uint32_t c = 0; c < p.kchunks; ++c) {
+                    tma_load_2d(bs + c * kChunk, &tx_hi, static_cast<int>(c * kBK), y, full(s));
+                    if (xlo) {
+                        tma_load_2d(bs + (p.kchunks + c) * kChunk, &tx_lo, static_cast<int>(c * kBK),
+                                    y, full(s));
+                    }
+                }
+                last_full[s] = full(s);
+                last_parity[s] = ph;
+                outstanding = min(outstanding + 1, S);
+            }
+        }
+        if (!ok) {
+            // Let every copy this thread issued land before the CTA exits (bounded).
+            for (std::uint32_t s = 0; s < outstanding; ++s) {
+                const std::uint64_t t0 = now_ns();
+                while (!mbar_try(last_full[s], last_parity[s]) && now_ns() - t0 < kWaitNs) {
+                }
+            }
+        }
+    } else if (warp == 1 && lane == 0) {
+        // MMA issuer.
+        std::uint32_t it = 0, acc_it = 0, item_idx = 0;
+        bool ok = true;
+        for (std::uint32_t item = blockIdx.x; ok && item < items; item += gridDim.x, ++item_idx) {
+            const std::uint32_t ch = item / p.qtiles;
+            const std::uint32_t row0 = ch * p.chunk_rows;
+            const std::uint32_t rows = min(p.chunk_rows, p.n - row0);
+            const std::uint32_t tiles = (rows + kBN - 1) / kBN;
+            if (!mbar_wait(a_full, item_idx & 1u, abort_flag)) {
+                fail();
+                ok = false;
+                break;
+            }
+            tc_fence_after();
+            for (std::uint32_t t = 0; t < tiles; ++t, ++it, ++acc_it) {
+                const std::uint32_t s = it % S;
+                const std::uint32_t b = acc_it & 1u;
+                if (!mbar_wait(tempty0 + 8 * b, ((acc_it >> 1) & 1u) ^ 1u, abort_flag) ||
+                    !mbar_wait(full(s), (it / S) & 1u, abort_flag)) {
+                    fail();
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const std::uint32_t d_tmem = tmem + b * kBN;
+                const std::uint32_t bs = b0 + s * stage_bytes;
+                for (std::uint32_t c = 0; c < p.kchunks; ++c) {
+                    for (std::uint32_t kk = 0; kk < kBK / 16; ++kk) {
+                        const std::uint32_t off = c * kChunk + kk * 32;
+                        const std::uint64_t ah = sw128_desc(a_hi + off);
+                        const std::uint64_t bh = sw128_desc(bs + off);
+                        mma_bf16(d_tmem, ah, bh, (c | kk) != 0 ? 1u : 0u);
+                        if (xlo) {
+                            mma_bf16(d_tmem, ah, sw128_desc(bs + p.kchunks * kChunk + off), 1u);
+                        }
+                        if (qlo) {
+                            mma_bf16(d_tmem, sw128_desc(a_lo + off), bh, 1u);
+                        }
+                    }
+                }
+                mma_commit(empty(s));
+                mma_commit(tfull0 + 8 * b);
+            }
+            if (ok) {
+                mma_commit(a_empty);
+            }
+        }
+        // Every MMA this thread issued has completed before TMEM is freed (bounded).
+        mma_commit(drain);
+        const std::uint64_t t0 = now_ns();
+        while (!mbar_try(drain, 0) && now_ns() - t0 < kWaitNs) {
+        }
+    } else if (warp >= 4) {
+        // Epilogue: thread e owns query row e of the tile (TMEM lane e).
+        const std::uint32_t e = threadIdx.x - 128;
+        const std::uint32_t lane_base = static_cast<std::uint32_t>((warp & 3) * 32) << 16;
+        std::uint32_t acc_it = 0;
+        for (std::uint32_t item = blockIdx.x; item < items; item += gridDim.x) {
+            const std::uint32_t qt = item % p.qtiles;
+            const std::uint32_t ch = item / p.qtiles;
+            const std::uint32_t row = qt * kBM + e;
+            const bool live = row < p.nq;
+            const float qn = live ? p.qnorm[row] : 0.0F;
+            const std::uint32_t row0 = ch * p.chunk_rows;
+            const std::uint32_t rows = min(p.chunk_rows, p.n - row0);
+            const std::uint32_t tiles = (rows + kBN - 1) / kBN;
+            std::uint32_t count = 0;
+            float thr_d = INFINITY;
+            std::uint32_t thr_i = kNoId;
+            bool ok = true;
+            for (std::uint32_t t = 0; t < tiles; ++t, ++acc_it) {
+                const std::uint32_t b = acc_it & 1u;
+                if (!mbar_wait(tfull0 + 8 * b, (acc_it >> 1) & 1u, abort_flag)) {
+                    fail();
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                for (std::uint32_t cc = 0; cc < kBN / 32; ++cc) {
+                    std::uint32_t r[32];
+                    tmem_ld32(tmem + lane_base + b * kBN + cc * 32, r);
+                    if (cc == kBN / 32 - 1) {
+                        tc_fence_before();
+                        mbar_arrive(tempty0 + 8 * b);
+                    }
+                    const std::uint32_t id0 = row0 + t * kBN + cc * 32;
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) {
+                        const std::uint32_t id = id0 + static_cast<std::uint32_t>(j);
+                        if (!live || id >= row0 + rows) {
+                            continue;
+                        }
+                        const float s = __uint_as_float(r[j]);
+                        const float d = p.metric == 0 ? __fmaf_rn(-2.0F, s, __fadd_rn(qn, __ldg(p.xnorm + id)))
+                                                      : __fsub_rn(1.0F, s);
+                        if (count < p.kc || closer(d, id, thr_d, thr_i)) {
+                            std::uint32_t pos = count < p.kc ? count : p.kc - 1;
+                            while (pos > 0 && closer(d, id, list_d[(pos - 1) * kBM + e],
+                                                     list_i[(pos - 1) * kBM + e])) {
+                                list_d[pos * kBM + e] = list_d[(pos - 1) * kBM + e];
+                                list_i[pos * kBM + e] = list_i[(pos - 1) * kBM + e];
+                                --pos;
+                            }
+                            list_d[pos * kBM + e] = d;
+                            list_i[pos * kBM + e] = id;
+                            if (count < p.kc) {
+                                ++count;
+                            }
+                            if (count == p.kc) {
+                                thr_d = list_d[(p.kc - 1) * kBM + e];
+                                thr_i = list_i[(p.kc - 1) * kBM + e];
+                            }
+                        }
+                    }
+                }
+            }
+            if (!ok) {
+                break;
+            }
+            if (live) {
+                const std::size_t at = (static_cast<std::size_t>(row) * p.nchunks + ch) * p.kc;
+                for (std::uint32_t i = 0; i < p.kc; ++i) {
+                    p.cand_d[at + i] = i < count ? list_d[i * kBM + e] : INFINITY;
+                    p.cand_ids[at + i] = i < count ? list_i[i * kBM + e] : kNoId;
+                }
+                p.cand_tau[static_cast<std::size_t>(row) * p.nchunks + ch] =
+                    count == p.kc ? thr_d : INFINITY;
+            }
+        }
+    }
+
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 1) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                     "r"(kTmemCols)
+                     : "memory");
+    }
+}
+
+// -------------------------------------------------------------------------------------------
+// Preparation: bf16 hi / lo split, norms, flags. One warp per row.
+
+__device__ __forceinline__ bool small_integer(float v) {
+    return v == rintf(v) && fabsf(v) <= 256.0F;
+}
+
+struct PrepOut {
+    __nv_bfloat16* hi;
+    __nv_bfloat16* lo;
+    float* norm;
+    float* normalized;        // FP32 rows as searched (queries only; may be null)
+    std::uint8_t* exact;      // per row: small-integer components (may be null)
+    std::uint8_t* valid;      // per row (queries only)
+    std::uint32_t* flags;     // bit 0: a nonzero lo part; bit 1: a row that is not small-integer
+    float* max_norm;          // max sqrt(norm) (as u32 bits, atomicMax)
+    std::uint32_t* status;    // queries: error code, first bad row
+};
+
+__global__ void prep_rows_kernel(const float* src, std::uint32_t src_stride, std::uint32_t rows,
+                                 std::uint32_t dim, std::uint32_t dk, std::uint32_t row32,
+                                 std::uint32_t metric, std::uint32_t check, PrepOut o) {
+    const int lane = threadIdx.x & 31;
+    const std::uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    extern __shared__ __align__(16) float qbuf[];
+    float* q = qbuf + (threadIdx.x >> 5) * row32;
+    for (std::uint32_t r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < rows; r += warps) {
+        const float* x = src + static_cast<std::size_t>(r) * src_stride;
+        bool bad = false;
+        for (std::uint32_t e = lane; e < row32; e += 32) {
+            const float v = e < dim ? x[e] : 0.0F;
+            bad |= !isfinite(v);
+            q[e] = v;
+        }
+        __syncwarp();
+        bool valid = true;
+        if (check && __any_sync(kFull, bad)) {
+            if (lane == 0) {
+                atomicCAS(o.status, 0u, 1u);
+                atomicMin(o.status + 1, r);
+            }
+            valid = false;
+        } else if (check && metric == 2) {
+            const float raw = warp_raw<kFP32, false>(q, reinterpret_cast<const unsigned char*>(q),
+                                                     dim, row32 * 4, lane);
+            const float n = sqrtf(raw);
+            if (!(n > 0.0F) || !isfinite(n)) {
+                if (lane == 0) {
+                    atomicCAS(o.status, 0u, 2u);
+                    atomicMin(o.status + 1, r);
+                }
+                valid = false;
+            } else {
+                __syncwarp();
+                for (std::uint32_t e = lane; e < dim; e += 32) {
+                    q[e] = __fdiv_rn(q[e], n);
+                }
+            }
+        }
+        __syncwarp();
+        bool has_lo = false, not_int = false;
+        for (std::uint32_t e = lane; e < dk; e += 32) {
+            const float v = valid && e < dim ? q[e] : 0.0F;
+            const __nv_bfloat16 h = __float2bfloat16_rn(v);
+            const __nv_bfloat16 l = __float2bfloat16_rn(v - __bfloat162float(h));
+            has_lo |= __bfloat162float(l) != 0.0F;
+            not_int |= !small_integer(v);
+            o.hi[static_cast<std::size_t>(r) * dk + e] = h;
+            o.lo[static_cast<std::size_t>(r) * dk + e] = l;
+            if (o.normalized != nullptr && e < row32) {
+                o.normalized[static_cast<std::size_t>(r) * row32 + e] = valid ? q[e] : 0.0F;
+            }
+        }
+        has_lo = __any_sync(kFull, has_lo);
+        not_int = __any_sync(kFull, not_int);
+        __syncwarp();
+        const float nrm = valid ? warp_raw<kFP32, false>(q, reinterpret_cast<const unsigned char*>(q),
+                                                         dim, row32 * 4, lane)
+                                : 0.0F;
+        if (lane == 0) {
+            o.norm[r] = nrm;
+            if (o.exact != nullptr) {
+                o.exact[r] = not_int ? 0 : 1;
+            }
+            if (o.valid != nullptr) {
+                o.valid[r] = valid ? 1 : 0;
+            }
+            const std::uint32_t f = (has_lo ? 1u : 0u) | (not_int ? 2u : 0u);
+            if (f != 0) {
+                atomicOr(o.flags, f);
+            }
+            atomicMax(reinterpret_cast<std::uint32_t*>(o.max_norm), __float_as_uint(sqrtf(nrm)));
+        }
+        __syncwarp();
+    }
+}
+
+// -------------------------------------------------------------------------------------------
+// Merge, exact re-rank, certification. One warp per query.
+
+struct MergeParams {
+    std::uint32_t nq, n, dim, row32, nchunks, kc, k, out_stride, metric, dk, terms;
+    const float* queries;          // normalized FP32 rows [nq][row32]
+    const std::uint8_t* valid;
+    const std::uint8_t* q_exact;
+    const float* qnorm;
+    const float* vectors;          // FP32 stored rows [n][row32]
+    std::uint32_t base_exact;      // every stored component a small integer
+    const float* xmax;             // max stored norm
+    const std::uint32_t* cand_ids;
+    const float* cand_d;
+    const float* cand_tau;
+    std::uint32_t* out_ids;
+    float* out_dists;
+    std::uint32_t* out_counts;
+    std::uint32_t* uncertified;    // [nq] rows, count in uncertified_count
+    std::uint32_t* uncertified_count;
+};
+
+template <bool kL2>
+__global__ void bf_tc_merge_kernel(const MergeParams p) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const std::uint32_t per_warp = p.row32 * 4 + p.kc * 16 + 128;
+    unsigned char* ws = sm + warp * per_warp;
+    float* q = reinterpret_cast<float*>(ws);
+    float* rd = reinterpret_cast<float*>(ws + p.row32 * 4);
+    std::uint32_t* rid = reinterpret_cast<std::uint32_t*>(ws + p.row32 * 4 + p.kc * 4);
+    float* ed = reinterpret_cast<float*>(ws + p.row32 * 4 + p.kc * 8);
+    std::uint32_t* eid = reinterpret_cast<std::uint32_t*>(ws + p.row32 * 4 + p.kc * 12);
+    int* ap = reinterpret_cast<int*>(ws + p.row32 * 4 + p.kc * 16);
+    const std::uint32_t row = blockIdx.x * (blockDim.x >> 5) + warp;
+    if (row >= p.nq) {
+        return;
+    }
+    std::uint32_t* oid = p.out_ids + static_cast<std::size_t>(row) * p.out_stride;
+    float* od = p.out_dists + static_cast<std::size_t>(row) * p.out_stride;
+    if (!p.valid[row]) {
+        for (std::uint32_t i = lane; i < p.out_stride; i += 32) {
+            oid[i] = kNoId;
+            od[i] = INFINITY;
+        }
+        if (lane == 0) {
+            p.out_counts[row] = 0;
+        }
+        return;
+    }
+    for (std::uint32_t e = lane; e < p.row32; e += 32) {
+        q[e] = p.queries[static_cast<std::size_t>(row) * p.row32 + e];
+    }
+    __syncwarp();
+    int r = 0;
+    float tau = INFINITY;
+    unsigned long long unused = 0;
+    for (std::uint32_t ch = 0; ch < p.nchunks; ++ch) {
+        const std::size_t at = (static_cast<std::size_t>(row) * p.nchunks + ch) * p.kc;
+        for (std::uint32_t j0 = 0; j0 < p.kc; j0 += 32) {
+            const std::uint32_t id = p.cand_ids[at + j0 + lane];
+            const float d = p.cand_d[at + j0 + lane];
+            merge_round(rd, rid, r, static_cast<int>(p.kc), d, id, id != kNoId, ap, lane, unused);
+        }
+        tau = fminf(tau, p.cand_tau[static_cast<std::size_t>(row) * p.nchunks + ch]);
+    }
+    if (r == static_cast<int>(p.kc)) {
+        tau = fminf(tau, rd[r - 1]);  // every candidate dropped here was at least this far
+    }
+    // Exact distances of the kept candidates, in the reference's order.
+    float my_d = INFINITY;
+    std::uint32_t my_id = kNoId;
+    int rr = 0;
+    for (int j0 = 0; j0 < r; j0 += 32) {
+        const int j = j0 + lane;
+        const bool valid = j < r;
+        if (valid) {
+            my_id = rid[j] & kIdMask;
+            my_d = lane_distance<kFP32, kL2>(
+                q, reinterpret_cast<const unsigned char*>(p.vectors + static_cast<std::size_t>(my_id) * p.row32),
+                p.dim, p.row32 * 4);
+        }
+        __syncwarp();
+        merge_round(ed, eid, rr, static_cast<int>(p.k), my_d, my_id, valid, ap, lane, unused);
+    }
+    const int cnt = rr;
+    // Certification: no excluded vector can have an exact distance at or below the k-th.
+    bool certified = true;
+    if (tau < INFINITY) {
+        if (cnt < static_cast<int>(p.k)) {
+            certified = false;
+        } else {
+            const float ek = ed[cnt - 1];
+            float eps;
+            if (p.base_exact && p.q_exact[row] && p.metric == 0) {
+                eps = tau * 0x1.0p-23F;  // exact arithmetic; one rounding above 2^24
+            } else {
+                const float a = sqrtf(p.qnorm[row]) + *p.xmax;
+                const float c = 0x1.0p-13F + static_cast<float>(p.terms * p.dk + 2 * p.dim + 8) * 0x1.0p-22F;
+                eps = c * a * a;
+            }
+            certified = ek < tau - eps;
+        }
+    }
+    for (std::uint32_t i = lane; i < p.out_stride; i += 32) {
+        if (static_cast<int>(i) < cnt) {
+            oid[i] = eid[i] & kIdMask;
+            od[i] = ed[i];
+        } else {
+            oid[i] = kNoId;
+            od[i] = INFINITY;
+        }
+    }
+    if (lane == 0) {
+        p.out_counts[row] = static_cast<std::uint32_t>(cnt);
+        if (!certified) {
+            const std::uint32_t at = atomicAdd(p.uncertified_count, 1u);
+            p.uncertified[at] = row;
+        }
+    }
+}
+
+// -------------------------------------------------------------------------------------------
+// Host side
+
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                 const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                 const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                 CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiled encoder() {
+    static EncodeTiled fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            return static_cast<EncodeTiled>(nullptr);
+        }
+        return reinterpret_cast<EncodeTiled>(f);
+    }();
+    return fn;
+}
+
+// A [rows][dk] bf16 row-major matrix as 64 x 128 boxes with 128-byte swizzling.
+bool make_map(CUtensorMap* map, const void* ptr, std::uint32_t rows, std::uint32_t dk) {
+    EncodeTiled enc = encoder();
+    if (enc == nullptr) {
+        return false;
+    }
+    const cuuint64_t dims[2] = {dk, rows};
+    const cuuint64_t strides[1] = {static_cast<cuuint64_t>(dk) * 2};
+    const cuuint32_t box[2] = {kBK, kBM};
+    const cuuint32_t estr[2] = {1, 1};
+    return enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(ptr), dims, strides, box,
+               estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+std::size_t align_up(std::size_t x, std::size_t a) { return (x + a - 1) / a * a; }
+
+struct Plan {
+    std::uint32_t dk, kchunks, kc, stages, qtiles, nchunks, chunk_rows;
+    std::uint32_t off_b, off_lists, off_bar;
+    std::size_t smem;
+    bool ok;
+};
+
+Plan make_plan(std::uint32_t nq, std::uint32_t n, std::uint32_t dim, std::uint32_t k, bool xlo,
+               int sms) {
+    Plan pl{};
+    pl.dk = static_cast<std::uint32_t>(align_up(dim, kBK));
+    pl.kchunks = pl.dk / kBK;
+    pl.kc = k <= 16 ? 32 : (k <= 48 ? 64 : 0);
+    pl.ok = pl.kc != 0 && pl.kchunks <= 4 && n >= 1;
+    if (!pl.ok) {
+        return pl;
+    }
+    const std::size_t a_bytes = 2 * pl.kchunks * kChunk;
+    const std::size_t stage = (xlo ? 2 : 1) * pl.kchunks * kChunk;
+    const std::size_t lists = static_cast<std::size_t>(pl.kc) * kBM * 8;
+    const std::size_t limit = 227 * 1024 - 1024 - 256;
+    std::uint32_t stages = 4;
+    while (stages > 1 && a_bytes + stages * stage + lists > limit) {
+        --stages;
+    }
+    if (a_bytes + stages * stage + lists > limit || stages < 2) {
+        pl.ok = false;
+        return pl;
+    }
+    pl.stages = stages;
+    pl.off_b = static_cast<std::uint32_t>(a_bytes);
+    pl.off_lists = static_cast<std::uint32_t>(a_bytes + stages * stage);
+    pl.off_bar = static_cast<std::uint32_t>(pl.off_lists + lists);
+    pl.smem = 1024 + pl.off_bar + 8 * (2 * stages) + 64 + 16;
+    pl.qtiles = (nq + kBM - 1) / kBM;
+    // Chunks of the stored rows: about 8 work items per SM, at least one tile each.
+    const std::uint32_t target = std::max<std::uint32_t>(1, (8u * sms + pl.qtiles - 1) / pl.qtiles);
+    std::uint32_t rows = static_cast<std::uint32_t>(align_up((n + target - 1) / target, kBN));
+    pl.chunk_rows = std::max<std::uint32_t>(rows, kBN);
+    pl.nchunks = (n + pl.chunk_rows - 1) / pl.chunk_rows;
+    return pl;
+}
+
+}  // namespace
+
+struct TcBase {
+    void* hi = nullptr;
+    void* lo = nullptr;
+    float* norm = nullptr;
+    void* flags = nullptr;   // [0] flags, [1] max norm bits
+    std::uint32_t n = 0, dk = 0;
+    bool has_lo = false, exact = false;
+    float max_norm = 0.0F;
+    CUtensorMap map_hi{}, map_lo{};
+    int device = 0;
+};
+
+void free_tc_base(TcBase* b) {
+    if (b == nullptr) {
+        return;
+    }
+    for (void* ptr : {b->hi, b->lo, static_cast<void*>(b->norm), b->flags}) {
+        if (ptr != nullptr) {
+            cudaFree(ptr);
+        }
+    }
+    delete b;
+}
+
+cudaError_t prepare_tc_base(const BaseView& v, cudaStream_t stream, TcBase** out) {
+    auto* b = new TcBase();
+    b->n = v.n;
+    b->dk = static_cast<std::uint32_t>(align_up(v.dim, kBK));
+    cudaGetDevice(&b->device);
+    const std::size_t elems = static_cast<std::size_t>(v.n) * b->dk;
+    cudaError_t err = cudaMalloc(&b->hi, elems * 2);
+    if (err == cudaSuccess) err = cudaMalloc(&b->lo, elems * 2);
+    if (err == cudaSuccess) err = cudaMalloc(&b->norm, static_cast<std::size_t>(v.n) * 4);
+    if (err == cudaSuccess) err = cudaMalloc(&b->flags, 16);
+    if (err == cudaSuccess) err = cudaMemsetAsync(b->flags, 0, 16, stream);
+    if (err != cudaSuccess) {
+        free_tc_base(b);
+        return err;
+    }
+    PrepOut o{};
+    o.hi = static_cast<__nv_bfloat16*>(b->hi);
+    o.lo = static_cast<__nv_bfloat16*>(b->lo);
+    o.norm = b->norm;
+    o.flags = static_cast<std::uint32_t*>(b->flags);
+    o.max_norm = reinterpret_cast<float*>(static_cast<std::uint32_t*>(b->flags) + 1);
+    const int warps = 8;
+    prep_rows_kernel<<<1184, warps * 32, warps * v.row32 * 4, stream>>>(
+        v.vectors, v.row32, v.n, v.dim, b->dk, v.row32, v.metric, 0, o);
+    err = cudaGetLastError();
+    std::uint32_t host_flags[2] = {0, 0};
+    if (err == cudaSuccess) err = cudaMemcpyAsync(host_flags, b->flags, 8, cudaMemcpyDeviceToHost, stream);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(stream);
+    if (err != cudaSuccess) {
+        free_tc_base(b);
+        return err;
+    }
+    b->has_lo = (host_flags[0] & 1u) != 0;
+    // Exact integer arithmetic needs 2 * dim * 256^2 <= 2^24.
+    b->exact = (host_flags[0] & 2u) == 0 && 2ull * v.dim * 65536ull <= (1ull << 24);
+    std::memcpy(&b->max_norm, &host_flags[1], 4);
+    if (!make_map(&b->map_hi, b->hi, v.n, b->dk) || !make_map(&b->map_lo, b->lo, v.n, b->dk)) {
+        free_tc_base(b);
+        return cudaErrorNotSupported;
+    }
+    *out = b;
+    return cudaSuccess;
+}
+
+std::size_t bruteforce_tc_workspace(std::uint32_t nq, std::uint32_t n, std::uint32_t dim,
+                                    std::uint32_t k) {
+    const std::uint32_t dk = static_cast<std::uint32_t>(align_up(dim, kBK));
+    const std::uint32_t row32 = static_cast<std::uint32_t>(align_up(dim, 4));
+    const std::size_t nqp = align_up(nq, kBM);
+    int device = 0, sms = 148;
+    cudaGetDevice(&device);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    const Plan pl = make_plan(nq, n, dim, k, true, sms);
+    const std::size_t chunks = pl.ok ? pl.nchunks : 1;
+    const std::size_t kc = pl.ok ? pl.kc : 32;
+    return 4 * nqp * dk                         // q hi + lo
+           + 4 * nqp * row32                    // normalized FP32 queries
+           + 4 * nqp * 3                        // norms, exact and valid flags
+           + nq * chunks * kc * 8 + nq * chunks * 4  // candidates
+           + 4 * nqp + 4096 + 16 * 256;         // uncertified rows, flags, alignment
+}
+
+cudaError_t launch_bruteforce_tc(const BruteArgs& a, const TcBase& b, void* workspace,
+                                 cudaStream_t stream, std::uint32_t* uncertified_out) {
+    if (a.nq == 0) {
+        return cudaSuccess;
+    }
+    int device = 0, sms = 148;
+    cudaGetDevice(&device);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    const std::uint32_t dim = a.base.dim, row32 = a.base.row32, nq = a.nq, n = a.base.n;
+    Plan pl = make_plan(nq, n, dim, a.k, b.has_lo, sms);
+    if (!pl.ok || a.k > n || a.qstride != dim) {
+        return launch_bruteforce_exact(a, stream);  // shapes this path does not cover
+    }
+    const std::size_t nqp = align_up(nq, kBM);
+    auto* w = static_cast<unsigned char*>(workspace);
+    std::size_t off = 0;
+    const auto take = [&](std::size_t bytes) {
+        unsigned char* p = w + off;
+        off = align_up(off + bytes, 256);
+        return p;
+    };
+    auto* q_hi = reinterpret_cast<__nv_bfloat16*>(take(nqp * pl.dk * 2));
+    auto* q_lo = reinterpret_cast<__nv_bfloat16*>(take(nqp * pl.dk * 2));
+    auto* qf = reinterpret_cast<float*>(take(nqp * row32 * 4));
+    auto* qnorm = reinterpret_cast<float*>(take(nqp * 4));
+    auto* q_exact = take(nqp);
+    auto* q_valid = take(nqp);
+    auto* cand_ids = reinterpret_cast<std::uint32_t*>(take(static_cast<std::size_t>(nq) * pl.nchunks * pl.kc * 4));
+    auto* cand_d = reinterpret_cast<float*>(take(static_cast<std::size_t>(nq) * pl.nchunks * pl.kc * 4));
+    auto* cand_tau = reinterpret_cast<float*>(take(static_cast<std::size_t>(nq) * pl.nchunks * 4));
+    auto* uncert = reinterpret_cast<std::uint32_t*>(take(nqp * 4));
+    auto* flags = reinterpret_cast<std::uint32_t*>(take(64));  // [0] query flags [1] max norm [2] error
+
+    cudaError_t err = cudaMemsetAsync(flags, 0, 64, stream);
+    if (err == cudaSuccess) err = cudaMemsetAsync(uncertified_out, 0, 4, stream);
+    if (err == cudaSuccess && nqp > nq) {
+        err = cudaMemsetAsync(q_hi + static_cast<std::size_t>(nq) * pl.dk, 0, (nqp - nq) * pl.dk * 2, stream);
+    }
+    if (err == cudaSuccess && nqp > nq) {
+        err = cudaMemsetAsync(q_lo + static_cast<std::size_t>(nq) * pl.dk, 0, (nqp - nq) * pl.dk * 2, stream);
+    }
+    if (err != cudaSuccess) {
+        return err;
+    }
+    PrepOut o{};
+    o.hi = q_hi;
+    o.lo = q_lo;
+    o.norm = qnorm;
+    o.normalized = qf;
+    o.exact = q_exact;
+    o.valid = q_valid;
+    o.flags = flags;
+    o.max_norm = reinterpret_cast<float*>(flags + 1);
+    o.status = a.status;
+    prep_rows_kernel<<<std::min<std::uint32_t>((nq + 7) / 8, 1184), 256, 8 * row32 * 4, stream>>>(
+        a.queries, a.qstride, nq, dim, pl.dk, row32, a.base.metric, 1, o);
+    if ((err = cudaGetLastError()) != cudaSuccess) {
+        return err;
+    }
+
+    CUtensorMap mq_hi, mq_lo;
+    if (!make_map(&mq_hi, q_hi, static_cast<std::uint32_t>(nqp), pl.dk) ||
+        !make_map(&mq_lo, q_lo, static_cast<std::uint32_t>(nqp), pl.dk)) {
+        return cudaErrorNotSupported;
+    }
+    TcParams p{};
+    p.nq = nq;
+    p.n = n;
+    p.dim = dim;
+    p.kchunks = pl.kchunks;
+    p.qtiles = pl.qtiles;
+    p.nchunks = pl.nchunks;
+    p.chunk_rows = pl.chunk_rows;
+    p.kc = pl.kc;
+    p.stages = pl.stages;
+    p.metric = a.base.metric == 0 ? 0u : 1u;
+    p.base_lo = b.has_lo ? 1u : 0u;
+    p.query_flags = flags;
+    p.qnorm = qnorm;
+    p.xnorm = b.norm;
+    p.cand_ids = cand_ids;
+    p.cand_d = cand_d;
+    p.cand_tau = cand_tau;
+    p.error = a.status;
+    p.off_b = pl.off_b;
+    p.off_lists = pl.off_lists;
+    p.off_bar = pl.off_bar;
+    err = cudaFuncSetAttribute(bf_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(pl.smem));
+    if (err != cudaSuccess) {
+        return err;
+    }
+    const std::uint32_t items = pl.qtiles * pl.nchunks;
+    const std::uint32_t grid = std::min<std::uint32_t>(items, static_cast<std::uint32_t>(sms));
+    bf_tc_kernel<<<grid, kThreads, pl.smem, stream>>>(mq_hi, mq_lo, b.map_hi, b.map_lo, p);
+    if ((err = cudaGetLastError()) != cudaSuccess) {
+        return err;
+    }
+
+    MergeParams m{};
+    m.nq = nq;
+    m.n = n;
+    m.dim = dim;
+    m.row32 = row32;
+    m.nchunks = pl.nchunks;
+    m.kc = pl.kc;
+    m.k = a.k;
+    m.out_stride = a.out_stride;
+    m.metric = a.base.metric;
+    m.dk = pl.dk;
+    m.terms = 3;  // hi*hi + hi*lo + lo*hi: the bound covers every term the data may need
+    m.queries = qf;
+    m.valid = q_valid;
+    m.q_exact = q_exact;
+    m.qnorm = qnorm;
+    m.vectors = a.base.vectors;
+    m.base_exact = b.exact ? 1u : 0u;
+    m.cand_ids = cand_ids;
+    m.cand_d = cand_d;
+    m.cand_tau = cand_tau;
+    m.out_ids = a.out_ids;
+    m.out_dists = a.out_dists;
+    m.out_counts = a.out_counts;
+    m.uncertified = uncert;
+    m.uncertified_count = uncertified_out;
+    // The stored vectors' largest norm, as the prep kernel left it in the base's flag words.
+    m.xmax = reinterpret_cast<const float*>(static_cast<const std::uint32_t*>(b.flags) + 1);
+    const int warps = 8;
+    const std::size_t msmem = static_cast<std::size_t>(warps) * (row32 * 4 + pl.kc * 16 + 128);
+    if (a.base.metric == 0) {
+        bf_tc_merge_kernel<true><<<(nq + warps - 1) / warps, warps * 32, msmem, stream>>>(m);
+    } else {
+        bf_tc_merge_kernel<false><<<(nq + warps - 1) / warps, warps * 32, msmem, stream>>>(m);
+    }
+    if ((err = cudaGetLastError()) != cudaSuccess) {
+        return err;
+    }
+
+    // Queries the tensor cores could not certify: the exact kernel on just those rows.
+    BruteArgs f = a;
+    f.rows = uncert;
+    f.nrows_device = uncertified_out;
+    if ((err = launch_bruteforce_exact(f, stream)) != cudaSuccess) {
+        return err;
+    }
+    return cudaSuccess;
 }
 
 }  // namespace vdx::dev

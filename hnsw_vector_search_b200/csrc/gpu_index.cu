@@ -38,14 +38,16 @@ struct DeviceBase {
     dev::BaseView view{};
     int device = 0;
     void* alloc = nullptr;
+    mutable dev::TcBase* tc = nullptr;  // the tensor-core path's preparation, made on first use
     ~DeviceBase() {
+        int prev = 0;
+        cudaGetDevice(&prev);
+        cudaSetDevice(device);
+        dev::free_tc_base(tc);
         if (alloc != nullptr) {
-            int prev = 0;
-            cudaGetDevice(&prev);
-            cudaSetDevice(device);
             cudaFree(alloc);
-            cudaSetDevice(prev);
         }
+        cudaSetDevice(prev);
     }
 };
 
@@ -172,6 +174,8 @@ void raise_status(std::uint32_t code, const char* where) {
             throw std::runtime_error(std::format("{}: the device graph holds an out-of-range link", where));
         case dev::kErrCapacity:
             throw std::invalid_argument(std::format("{}: ef exceeds the GPU search capacity", where));
+        case dev::kErrTimeout:
+            throw CudaError(std::format("{}: a device wait timed out", where));
         default:
             throw std::runtime_error(std::format("{}: device error {}", where, code));
     }
@@ -586,8 +590,15 @@ void BruteForceIndex::search_batch_into(MatrixView<float> queries, std::size_t k
     a.out_counts = ws.counts;
     a.status = ws.small;
     if (method == BruteMethod::TensorCore) {
+        {
+            const std::scoped_lock lock(*device_mutex_);
+            if (b.tc == nullptr) {
+                gpu::check(dev::prepare_tc_base(b.view, ws.stream, &b.tc), "tensor-core preparation");
+            }
+        }
         void* work = ws.scratch_bytes(dev::bruteforce_tc_workspace(a.nq, b.view.n, b.view.dim, a.k));
-        gpu::check(dev::launch_bruteforce_tc(a, work, ws.stream, ws.small + 8), "brute-force (tensor cores)");
+        gpu::check(dev::launch_bruteforce_tc(a, *b.tc, work, ws.stream, ws.small + 8),
+                   "brute-force (tensor cores)");
     } else {
         gpu::check(dev::launch_bruteforce_exact(a, ws.stream), "brute-force kernel");
     }

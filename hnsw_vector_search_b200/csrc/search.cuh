@@ -32,6 +32,7 @@ enum SearchError : std::uint32_t {
     kErrZeroCosine = 2,    // a cosine query cannot be normalized
     kErrBounds = 3,        // a link id out of range (a corrupted device graph)
     kErrCapacity = 4,      // ef exceeds the launch's result-list capacity
+    kErrTimeout = 5,       // a bounded device wait gave up (tensor-core brute force)
 };
 
 // The learned early-termination network (12 -> 64 -> 64 -> 1, ReLU, sigmoid), as the search

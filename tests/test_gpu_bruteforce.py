@@ -87,3 +87,40 @@ def test_errors(gpu):
     with pytest.raises(ValueError, match="NaN or inf"):
         bf.add(np.array([[np.nan, 0.0]], np.float32))
     assert len(bf) == 1
+
+
+@pytest.mark.parametrize("metric,make", [
+    (0, "sift"), (2, "glove"), (1, "scaled"), (0, "uniform")])
+def test_tensor_core_equals_exact_at_scale(gpu, metric, make):
+    """Many tiles and chunks: the tensor-core path (with certification and the exact fallback)
+    returns exactly the exact kernel's (= the reference's) ids and distance bits."""
+    from hnsw_vector_search_b200 import datasets as ds
+    if make == "sift":
+        base, queries = ds.config_sift_like(rows=40_000, n_queries=600)
+    elif make == "glove":
+        base, queries = ds.config_glove_like(rows=30_000, n_queries=400)
+    elif make == "scaled":
+        base, queries = ds.config_scaled_ip(rows=30_000, n_queries=400)
+    else:
+        base, queries = uniform_matrix(25_000, 100, 7), uniform_matrix(300, 100, 8)
+    bf = gpu.BruteForceIndex(base.shape[1], metric)
+    bf.add(base)
+    for k in (1, 10):
+        a = bf.search_batch(queries, k, method="exact")
+        b = bf.search_batch(queries, k, method="tensor_core")
+        np.testing.assert_array_equal(a[2], b[2])
+        np.testing.assert_array_equal(a[0], b[0])
+        np.testing.assert_array_equal(a[1].view(np.uint32), b[1].view(np.uint32))
+
+
+def test_tensor_core_matches_reference(gpu, orc):
+    from hnsw_vector_search_b200 import datasets as ds
+    base, queries = ds.config_sift_like(rows=20_000, n_queries=200)
+    ref = orc.RefBruteForce(128, 0)
+    ref.add(base)
+    bf = gpu.BruteForceIndex(128)
+    bf.add(base)
+    a = bf.search_batch(queries, 10, method="tensor_core")
+    b = ref.search_batch(queries, 10)
+    np.testing.assert_array_equal(a[0], b[0])
+    np.testing.assert_array_equal(a[1].view(np.uint32), b[1].view(np.uint32))
