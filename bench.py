@@ -108,7 +108,7 @@ class Clocks:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             threading.Thread(target=self._read, daemon=True).start()
         except FileNotFoundError:
@@ -254,12 +254,12 @@ def ground_truth(base, queries):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="vdx")
     ap.add_argument("--profile", action="store_true",
                     help="one search launch per warm-up step on the cached workload (for ncu)")
-    ap.add_argument("--mode", default="fp32", choices=["fp32", "bf16", "fp8"])
+    ap.add_argument("--mode", default="fp32", choices=["fp32", "bf16", "fp8", "bf_tc", "bf_exact"])
     ap.add_argument("--ef", type=int, default=32)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -390,6 +390,7 @@ def main():
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         e2e_total = float(t.item())
 
+    brute = bruteforce_section(v, torch, base, queries, dev) if rank == 0 else None
     if rank == 0:
         cpu = cpu_baseline(graph, queries, results["fp32"]["ef"])
     if pg is not None:
@@ -421,6 +422,7 @@ def main():
                     "d2h_bytes_per_step": int(nq * K * 8 + nq * 4)},
             "gpu_launches": args.steps,
             "clocks": clock_summary,
+            "bruteforce": brute,
         }
         print(json.dumps(line), flush=True)
     if pg is not None:
@@ -428,10 +430,77 @@ def main():
         pg.destroy_process_group()
 
 
+def bruteforce_section(v, torch, base, queries, dev) -> dict:
+    """Exact brute force of the 10,000 queries over the 1M vectors, k = 10: the tensor-core path
+    (tcgen05 GEMM + certified exact re-rank) against the exact CUDA-core kernel, timed with CUDA
+    events on the launching stream, results compared id for id and bit for bit."""
+    bf = v.BruteForceIndex(base.shape[1], "l2")
+    bf.add(base)
+    nq = len(queries)
+    q = torch.from_numpy(queries).to(dev)
+    out = {}
+    stream = torch.cuda.current_stream(dev)
+    res = {}
+    for method, reps in (("tensor_core", 5), ("exact", 1)):
+        ids = torch.empty((nq, K), dtype=torch.int32, device=dev)
+        d = torch.empty((nq, K), dtype=torch.float32, device=dev)
+        c = torch.empty(nq, dtype=torch.int32, device=dev)
+        work = torch.zeros(64, dtype=torch.int32, device=dev)
+        bf.search_batch_device(q, K, ids, d, c, work, method=method, stream=stream.cuda_stream)
+        torch.cuda.synchronize()
+        times = []
+        for _ in range(reps):
+            start = torch.cuda.Event(enable_timing=True)
+            end = torch.cuda.Event(enable_timing=True)
+            start.record(stream)
+            bf.search_batch_device(q, K, ids, d, c, work, method=method, stream=stream.cuda_stream)
+            end.record(stream)
+            end.synchronize()
+            times.append(start.elapsed_time(end))
+        res[method] = (ids.cpu().numpy(), d.cpu().numpy(), c.cpu().numpy(), float(np.median(times)),
+                       int(work[8].item()), int(work[0].item()))
+    tc, ex = res["tensor_core"], res["exact"]
+    n, dim = base.shape
+    dk = (dim + 63) // 64 * 64
+    fp32_flops = 2.0 * nq * n * dim
+    tensor_flops = 2.0 * ((nq + 127) // 128 * 128) * ((n + 127) // 128 * 128) * dk  # hi*hi only: integer data
+    peaks_f = ROOT / "MEASURED_PEAKS.json"
+    bf16_peak = float(json.loads(peaks_f.read_text())["bf16_tflops"]) if peaks_f.exists() else 1590.0
+    out = {"workload": f"{nq} x {n} x {dim} L2, k {K}",
+           "tensor_core_ms": tc[3], "exact_ms": ex[3],
+           "speedup_vs_exact": ex[3] / tc[3],
+           "uncertified_queries": tc[4], "status": [tc[5], ex[5]],
+           "identical_to_exact": bool(np.array_equal(tc[0], ex[0]) and
+                                      np.array_equal(tc[1].view(np.uint32), ex[1].view(np.uint32))),
+           "fp32_equivalent_tflops": fp32_flops / (tc[3] * 1e-3) / 1e12,
+           "tensor_tflops_pipeline": tensor_flops / (tc[3] * 1e-3) / 1e12,
+           "tensor_frac_of_measured_bf16_pipeline": tensor_flops / (tc[3] * 1e-3) / 1e12 / bf16_peak,
+           "note": "pipeline time: query prep + tcgen05 GEMM/epilogue + merge/re-rank + exact "
+                   "fallback for uncertified rows; the GEMM kernel's share is in profiles/"}
+    return out
+
+
 def profile(args, v, torch):
     """`warmup` + 1 launches of the search kernel on the cached 1M workload, nothing else on
     the GPU in between: the command the committed ncu summaries were captured from."""
     base, queries = workload()
+    if args.mode.startswith("bf_"):
+        bf = v.BruteForceIndex(base.shape[1], "l2")
+        bf.add(base)
+        dev = torch.device("cuda", 0)
+        q = torch.from_numpy(queries).to(dev)
+        nq = len(queries)
+        ids = torch.empty((nq, K), dtype=torch.int32, device=dev)
+        d = torch.empty((nq, K), dtype=torch.float32, device=dev)
+        c = torch.empty(nq, dtype=torch.int32, device=dev)
+        work = torch.zeros(64, dtype=torch.int32, device=dev)
+        method = "tensor_core" if args.mode == "bf_tc" else "exact"
+        for _ in range(args.warmup + 1):
+            bf.search_batch_device(q, K, ids, d, c, work, method=method)
+        torch.cuda.synchronize()
+        print(json.dumps({"profile": args.mode, "uncertified": int(work[8].item()),
+                          "status": int(work[0].item())}))
+        return
     ix = v.HnswIndex.load(reference_graph(base))
     o = {} if args.mode == "fp32" else {"precision": args.mode, "rerank": 40}
     ix.upload(0, args.mode)

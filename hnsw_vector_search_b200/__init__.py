@@ -86,6 +86,8 @@ def lib() -> ctypes.CDLL:
         "vdx_bf_add": (ctypes.c_int, [_P, _P, _U64, _U64]),
         "vdx_bf_size": (_U64, [_P]),
         "vdx_bf_search_batch": (ctypes.c_int, [_P, _P, _U64, _U64, _U64, _U32, _P, _P, _P]),
+        "vdx_bf_search_batch_device": (ctypes.c_int, [_P, _P, _U64, _U64, _U64, _U32, _P, _P, _P,
+                                                      _P, _P]),
         "vdx_host_l2": (_F, [_P, _P, _U64]),
         "vdx_host_ip": (_F, [_P, _P, _U64]),
         "vdx_xxh64": (_U64, [_P, _U64, _U64]),
@@ -279,6 +281,20 @@ class BruteForceIndex:
         _raise(lib().vdx_bf_search_batch(self._h, _ptr(q), nq, q.shape[1] if q.ndim == 2 else self._dim,
                                          kk, m, _ptr(ids), _ptr(dists), _ptr(counts)))
         return ids, dists, counts
+
+    def search_batch_device(self, queries, k: int, ids, dists, counts, work, method="exact",
+                            stream=0) -> None:
+        """Asynchronous device-buffer brute force (torch CUDA tensors)."""
+        m = {"exact": 0, "tensor_core": 1}[method]
+        _raise(lib().vdx_bf_search_batch_device(
+            self._h, queries.data_ptr(), queries.shape[0], queries.shape[1], k, m,
+            ids.data_ptr(), dists.data_ptr(), counts.data_ptr(), work.data_ptr(), stream))
+
+    @staticmethod
+    def last_uncertified() -> int:
+        out = np.zeros(16, np.uint64)
+        _raise(lib().vdx_last_stats(_ptr(out), 16))
+        return int(out[12])
 
     def search(self, query, k: int):
         ids, d, c = self.search_batch(np.asarray(query, np.float32).reshape(1, -1), k)

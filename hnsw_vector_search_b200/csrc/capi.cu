@@ -318,6 +318,21 @@ vdx_status vdx_bf_search_batch(const vdx_bruteforce* index, const float* queries
     });
 }
 
+vdx_status vdx_bf_search_batch_device(const vdx_bruteforce* index, const float* d_queries,
+                                      uint64_t nq, uint64_t dim, uint64_t k, uint32_t method,
+                                      uint32_t* d_ids, float* d_dists, uint32_t* d_counts,
+                                      uint32_t* d_work, void* stream) {
+    return guarded([&] {
+        require(index, "index");
+        require(d_work, "d_work");
+        if (method > 1) {
+            throw std::invalid_argument("unknown brute-force method");
+        }
+        index->index.search_batch_device(d_queries, nq, dim, k, d_ids, d_dists, d_counts, d_work,
+                                         static_cast<vdx::BruteMethod>(method), stream);
+    });
+}
+
 float vdx_host_l2(const float* a, const float* b, uint64_t dim) {
     return vdx::detail::l2_squared_raw(a, b, dim);
 }

@@ -609,7 +609,54 @@ void BruteForceIndex::search_batch_into(MatrixView<float> queries, std::size_t k
                "copy distances");
     gpu::check(cudaMemcpyAsync(counts, ws.counts, nq * 4, cudaMemcpyDeviceToHost, ws.stream), "copy counts");
     gpu::check(cudaStreamSynchronize(ws.stream), "brute force");
+    std::fill(std::begin(ws.last_stats), std::end(ws.last_stats), 0ULL);
+    ws.last_stats[0] = nq;
+    ws.last_stats[12] = method == BruteMethod::TensorCore ? ws.small_host[8] : 0;
     gpu::raise_status(ws.small_host[0], where);
+}
+
+void BruteForceIndex::search_batch_device(const float* d_queries, std::size_t nq, std::size_t dim,
+                                          std::size_t k, Id* d_ids, float* d_dists,
+                                          std::uint32_t* d_counts, std::uint32_t* d_work,
+                                          BruteMethod method, void* stream, int device) const {
+    const char* where = "BruteForceIndex::search";
+    detail::check_query_shape(where, {metric_, this->dim(), size()}, dim, k);
+    auto s = static_cast<cudaStream_t>(stream);
+    gpu::use_device(device);
+    gpu::check(cudaMemsetAsync(d_work, 0, 64 * 4, s), "reset work words");
+    gpu::check(cudaMemsetAsync(d_work + 1, 0xFF, 4, s), "reset work words");
+    if (nq == 0) {
+        return;
+    }
+    if (size() == 0) {
+        gpu::check(cudaMemsetAsync(d_counts, 0, nq * 4, s), "clear counts");
+        return;
+    }
+    const DeviceBase& b = device_base(device);
+    dev::BruteArgs a;
+    a.base = b.view;
+    a.queries = d_queries;
+    a.nq = static_cast<std::uint32_t>(nq);
+    a.qstride = static_cast<std::uint32_t>(dim);
+    a.k = static_cast<std::uint32_t>(k);
+    a.out_stride = static_cast<std::uint32_t>(k);
+    a.out_ids = d_ids;
+    a.out_dists = d_dists;
+    a.out_counts = d_counts;
+    a.status = d_work;
+    if (method == BruteMethod::TensorCore) {
+        gpu::Workspace& ws = gpu::workspace(device);
+        {
+            const std::scoped_lock lock(*device_mutex_);
+            if (b.tc == nullptr) {
+                gpu::check(dev::prepare_tc_base(b.view, s, &b.tc), "tensor-core preparation");
+            }
+        }
+        void* work = ws.scratch_bytes(dev::bruteforce_tc_workspace(a.nq, b.view.n, b.view.dim, a.k));
+        gpu::check(dev::launch_bruteforce_tc(a, *b.tc, work, s, d_work + 8), "brute-force (tensor cores)");
+    } else {
+        gpu::check(dev::launch_bruteforce_exact(a, s), "brute-force kernel");
+    }
 }
 
 std::vector<Neighbor> BruteForceIndex::search(std::span<const float> query, std::size_t k) const {

@@ -49,6 +49,13 @@ public:
                            std::uint32_t* counts, BruteMethod method = BruteMethod::Exact,
                            int device = 0, const char* where = "BruteForceIndex::search") const;
 
+    // The device-buffer form: queries, results and the work words (status, first failing row,
+    // uncertified count at word 8) in device memory, asynchronous on `stream`.
+    void search_batch_device(const float* d_queries, std::size_t nq, std::size_t dim,
+                             std::size_t k, Id* d_ids, float* d_dists, std::uint32_t* d_counts,
+                             std::uint32_t* d_work, BruteMethod method, void* stream,
+                             int device = 0) const;
+
     std::span<const float> vectors() const noexcept { return vectors_.data(); }
     const DeviceBase& device_base(int device) const;
 

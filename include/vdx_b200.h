@@ -65,7 +65,9 @@ typedef struct vdx_search_options {
 enum {
     VDX_STAT_QUERIES = 0, VDX_STAT_EXPANSIONS, VDX_STAT_DIST_LAYER0, VDX_STAT_DIST_UPPER,
     VDX_STAT_LINK_BYTES, VDX_STAT_ROW_BYTES, VDX_STAT_RERANK_BYTES, VDX_STAT_DUPLICATES,
-    VDX_STAT_PREFETCH_HITS, VDX_STAT_LEARNED_STOPS, VDX_STAT_COUNT
+    VDX_STAT_PREFETCH_HITS, VDX_STAT_LEARNED_STOPS, VDX_STAT_COUNT,
+    /* after a brute-force batch: queries the tensor-core path could not certify */
+    VDX_STAT_BF_UNCERTIFIED = 12
 };
 
 VDX_API const char* vdx_last_error(void);
@@ -165,6 +167,14 @@ VDX_API uint64_t vdx_bf_size(const vdx_bruteforce* index);
 VDX_API vdx_status vdx_bf_search_batch(const vdx_bruteforce* index, const float* queries,
                                        uint64_t nq, uint64_t dim, uint64_t k, uint32_t method,
                                        uint32_t* ids, float* dists, uint32_t* counts);
+
+/* The device-buffer form of vdx_bf_search_batch, asynchronous on `stream`: d_queries nq x dim,
+ * d_ids / d_dists nq x k, d_counts nq, d_work vdx_work_words() u32 ([0] error code, [1] first
+ * failing row, [8] number of queries the tensor-core path recomputed exactly). */
+VDX_API vdx_status vdx_bf_search_batch_device(const vdx_bruteforce* index, const float* d_queries,
+                                              uint64_t nq, uint64_t dim, uint64_t k,
+                                              uint32_t method, uint32_t* d_ids, float* d_dists,
+                                              uint32_t* d_counts, uint32_t* d_work, void* stream);
 
 /* --- Host helpers (the distance kernels' order, the file checksum) -------------------------- */
 
