@@ -150,7 +150,7 @@ struct TcParams {
     std::uint32_t base_lo;                // the stored vectors have nonzero lo parts
     const std::uint32_t* query_flags;     // bit 0: some query has a nonzero lo part
     const float* qnorm;                   // [nq]
-    const float* xnorm;                   // [n]
+    const float* xnorm;                   // [n rounded up to a tile]: the score bias
     std::uint32_t* cand_ids;              // [nq][nchunks][kc]
     float* cand_d;
     float* cand_tau;                      // [nq][nchunks]
@@ -334,21 +334,25 @@ __global__ void __launch_bounds__(kThreads, 1)
         while (!mbar_try(drain, 0) && now_ns() - t0 < kWaitNs) {
         }
     } else if (warp >= 4) {
-        // Epilogue: thread e owns query row e of the tile (TMEM lane e).
+        // Epilogue: thread e owns query row e of the tile (TMEM lane e). It works in score space,
+        // t = 2 q.x - ||x||^2 (L2) or t = q.x (inner product), larger is closer; the per-row
+        // bias (||x||^2, or 0; +inf for padding rows) is read 32 at a time with broadcast 16-byte
+        // loads, and a chunk of 32 scores enters the insertion path only if its best score can
+        // beat the list's current worst.
         const std::uint32_t e = threadIdx.x - 128;
         const std::uint32_t lane_base = static_cast<std::uint32_t>((warp & 3) * 32) << 16;
+        const bool l2 = p.metric == 0;
         std::uint32_t acc_it = 0;
         for (std::uint32_t item = blockIdx.x; item < items; item += gridDim.x) {
             const std::uint32_t qt = item % p.qtiles;
             const std::uint32_t ch = item / p.qtiles;
             const std::uint32_t row = qt * kBM + e;
             const bool live = row < p.nq;
-            const float qn = live ? p.qnorm[row] : 0.0F;
             const std::uint32_t row0 = ch * p.chunk_rows;
             const std::uint32_t rows = min(p.chunk_rows, p.n - row0);
             const std::uint32_t tiles = (rows + kBN - 1) / kBN;
             std::uint32_t count = 0;
-            float thr_d = INFINITY;
+            float thr = -INFINITY;  // the kc-th best score so far (-inf while the list is short)
             std::uint32_t thr_i = kNoId;
             bool ok = true;
             for (std::uint32_t t = 0; t < tiles; ++t, ++acc_it) {
@@ -367,32 +371,54 @@ __global__ void __launch_bounds__(kThreads, 1)
                         mbar_arrive(tempty0 + 8 * b);
                     }
                     const std::uint32_t id0 = row0 + t * kBN + cc * 32;
+                    const float4* bias4 = reinterpret_cast<const float4*>(p.xnorm + id0);
+                    float sc[32];
+                    float best = -INFINITY;
 #pragma unroll
+                    for (int q4 = 0; q4 < 8; ++q4) {
+                        const float4 bv = __ldg(bias4 + q4);
+                        const float bb[4] = {bv.x, bv.y, bv.z, bv.w};
+#pragma unroll
+                        for (int u = 0; u < 4; ++u) {
+                            const float sv = __uint_as_float(r[4 * q4 + u]);
+                            const float v = l2 ? __fmaf_rn(2.0F, sv, -bb[u]) : __fsub_rn(sv, bb[u]);
+                            sc[4 * q4 + u] = v;
+                            best = fmaxf(best, v);
+                        }
+                    }
+                    // Rows past the chunk end belong to the next chunk (never here: chunks are
+                    // whole tiles) or are padding (bias +inf, score -inf).
+                    if (!live || best < thr || (count == p.kc && best == thr && id0 > thr_i)) {
+                        continue;
+                    }
+#pragma unroll 1
                     for (int j = 0; j < 32; ++j) {
+                        const float v = sc[j];
                         const std::uint32_t id = id0 + static_cast<std::uint32_t>(j);
-                        if (!live || id >= row0 + rows) {
+                        const bool better = count < p.kc ? v > -INFINITY
+                                                         : (v > thr || (v == thr && id < thr_i));
+                        if (!better) {
                             continue;
                         }
-                        const float s = __uint_as_float(r[j]);
-                        const float d = p.metric == 0 ? __fmaf_rn(-2.0F, s, __fadd_rn(qn, __ldg(p.xnorm + id)))
-                                                      : __fsub_rn(1.0F, s);
-                        if (count < p.kc || closer(d, id, thr_d, thr_i)) {
-                            std::uint32_t pos = count < p.kc ? count : p.kc - 1;
-                            while (pos > 0 && closer(d, id, list_d[(pos - 1) * kBM + e],
-                                                     list_i[(pos - 1) * kBM + e])) {
-                                list_d[pos * kBM + e] = list_d[(pos - 1) * kBM + e];
-                                list_i[pos * kBM + e] = list_i[(pos - 1) * kBM + e];
-                                --pos;
+                        std::uint32_t pos = count < p.kc ? count : p.kc - 1;
+                        while (pos > 0) {
+                            const float pv = list_d[(pos - 1) * kBM + e];
+                            const std::uint32_t pi = list_i[(pos - 1) * kBM + e];
+                            if (!(v > pv || (v == pv && id < pi))) {
+                                break;
                             }
-                            list_d[pos * kBM + e] = d;
-                            list_i[pos * kBM + e] = id;
-                            if (count < p.kc) {
-                                ++count;
-                            }
-                            if (count == p.kc) {
-                                thr_d = list_d[(p.kc - 1) * kBM + e];
-                                thr_i = list_i[(p.kc - 1) * kBM + e];
-                            }
+                            list_d[pos * kBM + e] = pv;
+                            list_i[pos * kBM + e] = pi;
+                            --pos;
+                        }
+                        list_d[pos * kBM + e] = v;
+                        list_i[pos * kBM + e] = id;
+                        if (count < p.kc) {
+                            ++count;
+                        }
+                        if (count == p.kc) {
+                            thr = list_d[(p.kc - 1) * kBM + e];
+                            thr_i = list_i[(p.kc - 1) * kBM + e];
                         }
                     }
                 }
@@ -401,13 +427,16 @@ __global__ void __launch_bounds__(kThreads, 1)
                 break;
             }
             if (live) {
+                // Back to distances: d = ||q||^2 - t (L2) or 1 - t; order is preserved.
+                const float qn = p.qnorm[row];
                 const std::size_t at = (static_cast<std::size_t>(row) * p.nchunks + ch) * p.kc;
                 for (std::uint32_t i = 0; i < p.kc; ++i) {
-                    p.cand_d[at + i] = i < count ? list_d[i * kBM + e] : INFINITY;
+                    const float v = list_d[i * kBM + e];
+                    p.cand_d[at + i] = i < count ? (l2 ? __fsub_rn(qn, v) : __fsub_rn(1.0F, v)) : INFINITY;
                     p.cand_ids[at + i] = i < count ? list_i[i * kBM + e] : kNoId;
                 }
                 p.cand_tau[static_cast<std::size_t>(row) * p.nchunks + ch] =
-                    count == p.kc ? thr_d : INFINITY;
+                    count == p.kc ? (l2 ? __fsub_rn(qn, thr) : __fsub_rn(1.0F, thr)) : INFINITY;
             }
         }
     }
@@ -516,6 +545,15 @@ __global__ void prep_rows_kernel(const float* src, std::uint32_t src_stride, std
             atomicMax(reinterpret_cast<std::uint32_t*>(o.max_norm), __float_as_uint(sqrtf(nrm)));
         }
         __syncwarp();
+    }
+}
+
+// The epilogue's per-row score bias: ||x||^2 for L2, 0 for inner product, +inf past the end.
+__global__ void bias_kernel(const float* norm, float* bias, std::uint32_t n, std::uint32_t n_pad,
+                            std::uint32_t l2) {
+    const std::uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n_pad) {
+        bias[i] = i < n ? (l2 ? norm[i] : 0.0F) : INFINITY;
     }
 }
 
@@ -730,6 +768,7 @@ struct TcBase {
     void* lo = nullptr;
     float* norm = nullptr;
     void* flags = nullptr;   // [0] flags, [1] max norm bits
+    float* bias = nullptr;   // [n rounded up to a tile]: ||x||^2 (L2) or 0 (IP); +inf padding
     std::uint32_t n = 0, dk = 0;
     bool has_lo = false, exact = false;
     float max_norm = 0.0F;
@@ -741,7 +780,7 @@ void free_tc_base(TcBase* b) {
     if (b == nullptr) {
         return;
     }
-    for (void* ptr : {b->hi, b->lo, static_cast<void*>(b->norm), b->flags}) {
+    for (void* ptr : {b->hi, b->lo, static_cast<void*>(b->norm), b->flags, static_cast<void*>(b->bias)}) {
         if (ptr != nullptr) {
             cudaFree(ptr);
         }
@@ -755,9 +794,11 @@ cudaError_t prepare_tc_base(const BaseView& v, cudaStream_t stream, TcBase** out
     b->dk = static_cast<std::uint32_t>(align_up(v.dim, kBK));
     cudaGetDevice(&b->device);
     const std::size_t elems = static_cast<std::size_t>(v.n) * b->dk;
+    const std::size_t n_pad = align_up(v.n, kBN);
     cudaError_t err = cudaMalloc(&b->hi, elems * 2);
     if (err == cudaSuccess) err = cudaMalloc(&b->lo, elems * 2);
-    if (err == cudaSuccess) err = cudaMalloc(&b->norm, static_cast<std::size_t>(v.n) * 4);
+    if (err == cudaSuccess) err = cudaMalloc(&b->norm, n_pad * 4);
+    if (err == cudaSuccess) err = cudaMalloc(&b->bias, n_pad * 4);
     if (err == cudaSuccess) err = cudaMalloc(&b->flags, 16);
     if (err == cudaSuccess) err = cudaMemsetAsync(b->flags, 0, 16, stream);
     if (err != cudaSuccess) {
@@ -774,6 +815,11 @@ cudaError_t prepare_tc_base(const BaseView& v, cudaStream_t stream, TcBase** out
     prep_rows_kernel<<<1184, warps * 32, warps * v.row32 * 4, stream>>>(
         v.vectors, v.row32, v.n, v.dim, b->dk, v.row32, v.metric, 0, o);
     err = cudaGetLastError();
+    if (err == cudaSuccess) {
+        bias_kernel<<<(static_cast<unsigned>(n_pad) + 255) / 256, 256, 0, stream>>>(
+            b->norm, b->bias, v.n, static_cast<std::uint32_t>(n_pad), v.metric == 0 ? 1u : 0u);
+        err = cudaGetLastError();
+    }
     std::uint32_t host_flags[2] = {0, 0};
     if (err == cudaSuccess) err = cudaMemcpyAsync(host_flags, b->flags, 8, cudaMemcpyDeviceToHost, stream);
     if (err == cudaSuccess) err = cudaStreamSynchronize(stream);
@@ -890,7 +936,7 @@ cudaError_t launch_bruteforce_tc(const BruteArgs& a, const TcBase& b, void* work
     p.base_lo = b.has_lo ? 1u : 0u;
     p.query_flags = flags;
     p.qnorm = qnorm;
-    p.xnorm = b.norm;
+    p.xnorm = b.bias;
     p.cand_ids = cand_ids;
     p.cand_d = cand_d;
     p.cand_tau = cand_tau;
