@@ -14,6 +14,7 @@
 #include "../host/src/internal.hpp"
 #include "capi_internal.hpp"
 #include "gpu_runtime.cuh"
+#include "mlp.cuh"
 #include "search.cuh"
 
 namespace {
@@ -277,6 +278,79 @@ vdx_status vdx_search_batch_device(const vdx_index* index, const float* d_querie
         const uint64_t cap = std::min<uint64_t>(std::max<uint64_t>(ef_uniform, kk), h.size());
         const vdx::dev::SearchPlan plan = vdx::dev::default_plan(g.view, static_cast<uint32_t>(cap));
         vdx::gpu::check(vdx::dev::launch_search(a, plan, s), "search kernel");
+    });
+}
+
+vdx_status vdx_index_set_stop_model(vdx_index* index, const float* weights, const float* mean,
+                                    const float* inv_std, const float* proj) {
+    return guarded([&] {
+        require(index, "index");
+        require(weights, "weights");
+        require(mean, "mean");
+        require(inv_std, "inv_std");
+        require(proj, "proj");
+        const std::size_t dim = index->index.dim();
+        vdx::StopModel m;
+        m.weights.assign(weights, weights + vdx::dev::kStopParams);
+        m.mean.assign(mean, mean + vdx::dev::kStopFeatures);
+        m.inv_std.assign(inv_std, inv_std + vdx::dev::kStopFeatures);
+        m.proj.assign(proj, proj + 4 * dim);
+        index->index.set_stop_model(std::move(m));
+    });
+}
+
+vdx_status vdx_stop_trace(const vdx_index* index, const float* queries, uint64_t nq, uint64_t dim,
+                          const uint32_t* truth, uint64_t truth_k, uint64_t k, uint64_t ef,
+                          const float* proj, uint64_t max_points, float* features, uint8_t* hits,
+                          uint32_t* points, uint8_t* final_hits, int32_t device) {
+    return guarded([&] {
+        require(index, "index");
+        require(proj, "proj");
+        if (nq > 0) {
+            require(queries, "queries");
+            require(truth, "truth");
+        }
+        index->index.trace_search(
+            vdx::MatrixView<float>(std::span<const float>(queries, nq * dim), dim == 0 ? 1 : dim),
+            truth, truth_k, k, ef, proj, max_points, features, hits, points, final_hits, device);
+    });
+}
+
+vdx_status vdx_mlp_train(const float* x, const float* y, uint64_t n, uint32_t epochs, uint64_t batch,
+                         float lr, uint64_t seed, float* weights, float* mean, float* inv_std,
+                         float* loss_per_epoch) {
+    return guarded([&] {
+        require(x, "x");
+        require(y, "y");
+        require(weights, "weights");
+        vdx::dev::MlpTrainConfig cfg;
+        cfg.epochs = static_cast<int>(epochs);
+        cfg.batch = batch;
+        cfg.lr = lr;
+        cfg.seed = seed;
+        vdx::gpu::use_device(0);
+        vdx::dev::mlp_train(x, y, n, cfg, weights, mean, inv_std, loss_per_epoch);
+    });
+}
+
+vdx_status vdx_mlp_gradient(const float* x, const float* y, uint64_t n, const float* weights,
+                            float* grad, float* loss) {
+    return guarded([&] {
+        require(x, "x");
+        require(weights, "weights");
+        require(grad, "grad");
+        vdx::gpu::use_device(0);
+        vdx::dev::mlp_gradient(x, y, n, weights, grad, loss);
+    });
+}
+
+vdx_status vdx_mlp_probabilities(const float* x, uint64_t n, const float* weights, const float* mean,
+                                 const float* inv_std, float* prob) {
+    return guarded([&] {
+        require(x, "x");
+        require(weights, "weights");
+        vdx::gpu::use_device(0);
+        vdx::dev::mlp_probabilities(x, n, weights, mean, inv_std, prob);
     });
 }
 

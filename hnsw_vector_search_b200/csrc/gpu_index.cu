@@ -27,6 +27,7 @@
 #include "bruteforce.cuh"
 #include "common.cuh"
 #include "gpu_runtime.cuh"
+#include "mlp.cuh"
 #include "search.cuh"
 #include "vdx/brute_force.hpp"
 #include "vdx/device.hpp"
@@ -393,6 +394,47 @@ const DeviceGraph* HnswIndex::uploaded_graph(int device, Precision precision) co
     return slot < device_.size() ? device_[slot].get() : nullptr;
 }
 
+void HnswIndex::set_stop_model(StopModel model) {
+    if (model.weights.size() != static_cast<std::size_t>(dev::kStopParams) ||
+        model.mean.size() != static_cast<std::size_t>(dev::kStopFeatures) ||
+        model.inv_std.size() != static_cast<std::size_t>(dev::kStopFeatures) ||
+        model.proj.size() != 4 * dim()) {
+        throw std::invalid_argument(std::format(
+            "HnswIndex::set_stop_model: expected {} weights, 12 means, 12 scales and 4 x {} "
+            "projections",
+            dev::kStopParams, dim()));
+    }
+    if (!device_mutex_) {
+        device_mutex_ = std::make_unique<std::mutex>();
+    }
+    const std::scoped_lock lock(*device_mutex_);
+    stop_model_ = std::move(model);
+    stop_net_.clear();
+}
+
+namespace {
+
+const dev::DeviceStopNet& stop_net_for(const HnswIndex& ix, std::mutex& m,
+                                       std::vector<std::shared_ptr<dev::DeviceStopNet>>& nets,
+                                       int device, const char* where) {
+    const std::scoped_lock lock(m);
+    if (!ix.has_stop_model()) {
+        throw std::invalid_argument(std::format("{}: learned_stop needs a model (set_stop_model)", where));
+    }
+    if (nets.size() <= static_cast<std::size_t>(device)) {
+        nets.resize(device + 1);
+    }
+    if (!nets[device]) {
+        const StopModel& sm = ix.stop_model();
+        nets[device] = dev::upload_stop_net(sm.weights.data(), sm.mean.data(), sm.inv_std.data(),
+                                            sm.proj.data(), static_cast<std::uint32_t>(ix.dim()),
+                                            round_up(static_cast<std::uint32_t>(ix.dim()), 4), device);
+    }
+    return *nets[device];
+}
+
+}  // namespace
+
 void HnswIndex::search_batch_into(MatrixView<float> queries, std::size_t k, std::size_t ef,
                                   Id* ids, float* distances, std::uint32_t* counts,
                                   const SearchOptions& options, const char* where) const {
@@ -434,6 +476,12 @@ void HnswIndex::search_batch_into(MatrixView<float> queries, std::size_t k, std:
     a.rerank = options.precision == Precision::FP32 ? 0U
                                                     : (options.rerank > 0 ? options.rerank
                                                                           : static_cast<std::uint32_t>(4 * k));
+    if (options.learned_stop) {
+        const dev::DeviceStopNet& net = stop_net_for(*this, *device_mutex_, stop_net_, options.device, where);
+        a.stop = net.view;
+        a.stop_enabled = &net;
+        a.stop_threshold = options.stop_threshold;
+    }
     const std::size_t ef_eff = std::min<std::size_t>(std::max(ef, k), size());
     dev::SearchPlan plan = dev::default_plan(dg.view, static_cast<std::uint32_t>(ef_eff));
     gpu::check(dev::launch_search(a, plan, ws.stream), "search kernel");
@@ -445,6 +493,81 @@ void HnswIndex::search_batch_into(MatrixView<float> queries, std::size_t k, std:
     gpu::check(cudaMemcpyAsync(counts, ws.counts, nq * 4, cudaMemcpyDeviceToHost, ws.stream), "copy counts");
     gpu::check(cudaStreamSynchronize(ws.stream), "search");
     std::memcpy(ws.last_stats, ws.small_host + 16, sizeof ws.last_stats);
+    gpu::raise_status(ws.small_host[0], where);
+}
+
+void HnswIndex::trace_search(MatrixView<float> queries, const Id* truth, std::size_t truth_k,
+                             std::size_t k, std::size_t ef, const float* proj,
+                             std::size_t max_points, float* features, std::uint8_t* hits,
+                             std::uint32_t* points, std::uint8_t* final_hits, int device) const {
+    const char* where = "HnswIndex::trace_search";
+    detail::check_query_shape(where, {metric_, dim(), size()}, queries.dim(), k);
+    if (k > 32 || truth_k > 32) {
+        throw std::invalid_argument(std::format("{}: k and truth_k must be at most 32", where));
+    }
+    const std::size_t nq = queries.rows();
+    if (nq == 0 || size() == 0) {
+        std::fill(points, points + nq, 0U);
+        std::fill(final_hits, final_hits + nq, std::uint8_t{0});
+        return;
+    }
+    const DeviceGraph& dg = device_graph(device, Precision::FP32);
+    gpu::Workspace& ws = gpu::workspace(device);
+    ws.reserve(nq, dim(), k);
+    const std::uint32_t row32 = round_up(static_cast<std::uint32_t>(dim()), 4);
+    // Temporary trace buffers (training only, not the query path).
+    struct Buffer {
+        void* p = nullptr;
+        Buffer(std::size_t bytes, const char* what) : p(gpu::device_alloc(bytes, what)) {}
+        ~Buffer() { cudaFree(p); }
+        Buffer(const Buffer&) = delete;
+        Buffer& operator=(const Buffer&) = delete;
+    };
+    const std::size_t fbytes = nq * max_points * dev::kStopFeatures * 4;
+    const Buffer dfeat(fbytes, "trace features");
+    const Buffer dhits(nq * max_points, "trace hits");
+    const Buffer dpoints(nq * 4, "trace points");
+    const Buffer dfinal(nq, "trace final hits");
+    const Buffer dtruth(nq * truth_k * 4, "trace truth");
+    const Buffer dproj(4ull * row32 * 4, "trace projections");
+    std::vector<float> proj_rows(4ull * row32, 0.0F);
+    for (int i = 0; i < 4; ++i) {
+        std::memcpy(proj_rows.data() + i * row32, proj + i * dim(), dim() * 4);
+    }
+    gpu::check(cudaMemcpyAsync(ws.queries, queries.data().data(), queries.data().size_bytes(),
+                               cudaMemcpyHostToDevice, ws.stream), "copy queries");
+    gpu::check(cudaMemcpyAsync(dtruth.p, truth, nq * truth_k * 4, cudaMemcpyHostToDevice, ws.stream),
+               "copy truth");
+    gpu::check(cudaMemcpyAsync(dproj.p, proj_rows.data(), proj_rows.size() * 4,
+                               cudaMemcpyHostToDevice, ws.stream), "copy projections");
+    gpu::reset_small(ws);
+    dev::SearchArgs a;
+    a.g = dg.view;
+    a.queries = ws.queries;
+    a.nq = static_cast<std::uint32_t>(nq);
+    a.qstride = static_cast<std::uint32_t>(dim());
+    a.k = static_cast<std::uint32_t>(k);
+    a.ef = static_cast<std::uint32_t>(ef);
+    a.out_stride = static_cast<std::uint32_t>(k);
+    a.out_ids = ws.ids;
+    a.out_dists = ws.dists;
+    a.out_counts = ws.counts;
+    a.status = ws.small;
+    a.claim = ws.small + 2;
+    a.stop.proj = static_cast<const float*>(dproj.p);
+    a.trace = {static_cast<const std::uint32_t*>(dtruth.p), static_cast<std::uint32_t>(truth_k),
+               static_cast<std::uint32_t>(max_points), static_cast<float*>(dfeat.p),
+               static_cast<std::uint8_t*>(dhits.p), static_cast<std::uint32_t*>(dpoints.p),
+               static_cast<std::uint8_t*>(dfinal.p)};
+    const std::size_t ef_eff = std::min<std::size_t>(std::max(ef, k), size());
+    dev::SearchPlan plan = dev::default_plan(dg.view, static_cast<std::uint32_t>(ef_eff));
+    gpu::check(dev::launch_search(a, plan, ws.stream), "trace kernel");
+    gpu::check(cudaMemcpyAsync(features, dfeat.p, fbytes, cudaMemcpyDeviceToHost, ws.stream), "copy features");
+    gpu::check(cudaMemcpyAsync(hits, dhits.p, nq * max_points, cudaMemcpyDeviceToHost, ws.stream), "copy hits");
+    gpu::check(cudaMemcpyAsync(points, dpoints.p, nq * 4, cudaMemcpyDeviceToHost, ws.stream), "copy points");
+    gpu::check(cudaMemcpyAsync(final_hits, dfinal.p, nq, cudaMemcpyDeviceToHost, ws.stream), "copy final");
+    gpu::check(cudaMemcpyAsync(ws.small_host, ws.small, 256, cudaMemcpyDeviceToHost, ws.stream), "status");
+    gpu::check(cudaStreamSynchronize(ws.stream), "trace");
     gpu::raise_status(ws.small_host[0], where);
 }
 

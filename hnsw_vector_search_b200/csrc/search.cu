@@ -123,6 +123,88 @@ __device__ __forceinline__ int first_unexpanded(const std::uint32_t* rid, int fr
     return r;
 }
 
+// ---------------------------------------------------------------------------------------------
+// Learned early termination: features and the network, evaluated by a whole warp (every lane
+// computes the same features from shared memory; the two hidden layers spread over the lanes).
+
+constexpr int kFeatures = 12;
+constexpr int kHidden = 64;
+constexpr int kHist = 32;  // ring of the k-th distance after each expansion
+
+__device__ __forceinline__ float sgnlog(float x) { return copysignf(log1pf(fabsf(x)), x); }
+
+// The 12 features of a query's search state after `hops` expansions (the model's inputs):
+//   0 log(1 + |q|)                      1 signed log of the layer-0 entry distance
+//   2 log(1 + (d_k - d_1) / |d_1|)      3..5 relative drop of d_k over the last 4 / 8 / 16
+//   6 log(1 + hops)                     7 log(1 + |R| / k)          8..11 query projections
+__device__ __forceinline__ void stop_features(float* f, float qlen, float d_entry, const float* proj,
+                                              const float* rd, int r, int k, const float* hist,
+                                              int hops) {
+    const int kk = r < k ? r : k;
+    const float d1 = rd[0];
+    const float dk = rd[kk - 1];
+    f[0] = log1pf(qlen);
+    f[1] = sgnlog(d_entry);
+    f[2] = log1pf(fmaxf(dk - d1, 0.0F) / (fabsf(d1) + 1e-3F * (1.0F + fabsf(dk))));
+    const int ws[3] = {4, 8, 16};
+#pragma unroll
+    for (int w = 0; w < 3; ++w) {
+        const int back = hops - 1 - ws[w];
+        const float prev = hist[(back > 0 ? back : 0) & (kHist - 1)];
+        const float drop = (prev - dk) / (fabsf(dk) + 1e-6F * (1.0F + fabsf(dk)));
+        f[3 + w] = fminf(fmaxf(drop, -10.0F), 10.0F);
+    }
+    f[6] = log1pf(static_cast<float>(hops));
+    f[7] = log1pf(static_cast<float>(r) / static_cast<float>(k));
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        f[8 + i] = proj[i];
+    }
+}
+
+__device__ __forceinline__ float bf16_bits(std::uint16_t b) {
+    return __uint_as_float(static_cast<std::uint32_t>(b) << 16);
+}
+
+// P(converged) of the network for features f (identical in every lane); h1 is 64 floats of
+// per-warp shared scratch.
+__device__ __forceinline__ float stop_probability(const StopNetView& net, const float* f, float* h1,
+                                                  int lane) {
+    float x[kFeatures];
+#pragma unroll
+    for (int c = 0; c < kFeatures; ++c) {
+        x[c] = (f[c] - net.mean[c]) * net.inv_std[c];
+    }
+    float a0 = net.b1[lane];
+    float a1 = net.b1[lane + 32];
+#pragma unroll
+    for (int c = 0; c < kFeatures; ++c) {
+        a0 = fmaf(bf16_bits(net.w1[lane * kFeatures + c]), x[c], a0);
+        a1 = fmaf(bf16_bits(net.w1[(lane + 32) * kFeatures + c]), x[c], a1);
+    }
+    __syncwarp();
+    h1[lane] = fmaxf(a0, 0.0F);
+    h1[lane + 32] = fmaxf(a1, 0.0F);
+    __syncwarp();
+    float z0 = net.b2[lane];
+    float z1 = net.b2[lane + 32];
+    const std::uint16_t* r0 = net.w2 + lane * kHidden;
+    const std::uint16_t* r1 = net.w2 + (lane + 32) * kHidden;
+#pragma unroll 8
+    for (int i = 0; i < kHidden; ++i) {
+        const float h = h1[i];
+        z0 = fmaf(bf16_bits(r0[i]), h, z0);
+        z1 = fmaf(bf16_bits(r1[i]), h, z1);
+    }
+    float part = bf16_bits(net.w3[lane]) * fmaxf(z0, 0.0F) + bf16_bits(net.w3[lane + 32]) * fmaxf(z1, 0.0F);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        part += __shfl_xor_sync(kFull, part, o);
+    }
+    const float logit = part + net.b3[0];
+    return 1.0F / (1.0F + __expf(-logit));
+}
+
 template <int P, bool kL2>
 __global__ void __launch_bounds__(256) search_kernel(const SearchArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -137,8 +219,12 @@ __global__ void __launch_bounds__(256) search_kernel(const SearchArgs a) {
     unsigned char* rows = ws + a.off_rows;
     std::uint32_t* fresh = reinterpret_cast<std::uint32_t*>(ws + a.off_fresh);
     int* ap = reinterpret_cast<int*>(ws + a.off_ap);
+    float* hist = reinterpret_cast<float*>(ws + a.off_hist);  // kHist k-th distances
+    float* h1 = hist + kHist;                                 // kHidden network scratch
 
     const DeviceGraphView& g = a.g;
+    const bool learned = a.stop_enabled != nullptr;
+    const bool tracing = a.trace.truth != nullptr;
     const auto* vecs = static_cast<const unsigned char*>(g.vectors);
     const std::uint32_t nq = a.nq_device != nullptr ? *a.nq_device : a.nq;
     const std::uint32_t hmask = a.hash_slots - 1;
@@ -147,7 +233,7 @@ __global__ void __launch_bounds__(256) search_kernel(const SearchArgs a) {
     const int shift = chunk_shift(g.row_bytes);
 
     unsigned long long c_exp = 0, c_d0 = 0, c_du = 0, c_lb = 0, c_rb = 0, c_rr = 0, c_dup = 0,
-                       c_pf = 0, c_q = 0;
+                       c_pf = 0, c_q = 0, c_stop = 0;
 
     for (;;) {
         std::uint32_t qi = 0;
@@ -215,6 +301,20 @@ __global__ void __launch_bounds__(256) search_kernel(const SearchArgs a) {
             __syncwarp();
         }
         ++c_q;
+        float qlen = 0.0F;
+        float proj[4] = {0.0F, 0.0F, 0.0F, 0.0F};
+        if (learned || tracing) {
+            qlen = sqrtf(warp_raw<kFP32, false>(q, reinterpret_cast<const unsigned char*>(q), g.dim,
+                                                g.row32 * 4, lane));
+            const float inv = 1.0F / fmaxf(qlen, 1e-20F);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                proj[i] = inv * warp_raw<kFP32, false>(
+                                    q, reinterpret_cast<const unsigned char*>(a.stop.proj + i * g.row32),
+                                    g.dim, g.row32 * 4, lane);
+            }
+        }
+        std::uint32_t trace_points = 0;
 
         // 2. Entry point and greedy descent.
         std::uint32_t cur = g.entry;
@@ -305,6 +405,8 @@ __global__ void __launch_bounds__(256) search_kernel(const SearchArgs a) {
         int scan = 0;
         int slot = 0;
         std::uint32_t prefetched = kNoId;
+        const float d_entry = curd;
+        int hops = 0;
         for (std::uint32_t step = 0; step <= g.n; ++step) {
             const int p = first_unexpanded(rid, scan, r, lane);
             if (p >= r) {
@@ -385,6 +487,46 @@ __global__ void __launch_bounds__(256) search_kernel(const SearchArgs a) {
                 scan = min(scan, low);
             }
             slot ^= 1;
+            ++hops;
+            if (learned || tracing) {
+                const int kk = r < static_cast<int>(k) ? r : static_cast<int>(k);
+                if (lane == 0) {
+                    hist[(hops - 1) & (kHist - 1)] = rd[kk - 1];
+                }
+                __syncwarp();
+                if ((hops & 7) == 0) {
+                    float f[kFeatures];
+                    stop_features(f, qlen, d_entry, proj, rd, r, static_cast<int>(k), hist, hops);
+                    if (tracing && trace_points < a.trace.max_points) {
+                        const std::size_t at = static_cast<std::size_t>(qi) * a.trace.max_points + trace_points;
+                        if (lane < kFeatures) {
+                            float v = f[0];
+#pragma unroll
+                            for (int c = 1; c < kFeatures; ++c) {
+                                v = lane == c ? f[c] : v;
+                            }
+                            a.trace.features[at * kFeatures + lane] = v;
+                        }
+                        const std::uint32_t my = lane < kk ? (rid[lane] & kIdMask) : kNoId;
+                        bool hit = false;
+                        for (std::uint32_t t = 0; t < a.trace.truth_k; ++t) {
+                            hit |= my == a.trace.truth[static_cast<std::size_t>(qi) * a.trace.truth_k + t];
+                        }
+                        const int hits = __popc(__ballot_sync(kFull, hit && my != kNoId));
+                        if (lane == 0) {
+                            a.trace.hits[at] = static_cast<std::uint8_t>(hits);
+                        }
+                        ++trace_points;
+                    }
+                    if (learned && hops >= static_cast<int>(a.stop_min_hops) && r >= static_cast<int>(k)) {
+                        const float pr = stop_probability(a.stop, f, h1, lane);
+                        if (pr >= a.stop_threshold) {
+                            ++c_stop;
+                            break;
+                        }
+                    }
+                }
+            }
         }
         cp_async_wait<0>();  // a prefetch may still be in flight
         __syncwarp();
@@ -440,6 +582,18 @@ __global__ void __launch_bounds__(256) search_kernel(const SearchArgs a) {
         if (lane == 0) {
             a.out_counts[qi] = static_cast<std::uint32_t>(cnt);
         }
+        if (tracing) {
+            const std::uint32_t my = lane < cnt ? (rid[lane] & kIdMask) : kNoId;
+            bool hit = false;
+            for (std::uint32_t t = 0; t < a.trace.truth_k; ++t) {
+                hit |= my == a.trace.truth[static_cast<std::size_t>(qi) * a.trace.truth_k + t];
+            }
+            const int hits = __popc(__ballot_sync(kFull, hit && my != kNoId));
+            if (lane == 0) {
+                a.trace.final_hits[qi] = static_cast<std::uint8_t>(hits);
+                a.trace.points[qi] = trace_points;
+            }
+        }
         __syncwarp();
     }
 
@@ -453,6 +607,7 @@ __global__ void __launch_bounds__(256) search_kernel(const SearchArgs a) {
         atomicAdd(a.stats + kStatRerankBytes, c_rr);
         atomicAdd(a.stats + kStatDuplicates, c_dup);
         atomicAdd(a.stats + kStatPrefetchHits, c_pf);
+        atomicAdd(a.stats + kStatLearnedStops, c_stop);
     }
 }
 
@@ -515,7 +670,7 @@ std::size_t plan_search(SearchArgs& a, const SearchPlan& plan) {
     a.off_ap = off;
     off += 32 * 4;
     a.off_hist = off;
-    off += 16 * 4;
+    off += (kHist + kHidden) * 4;
     a.warp_bytes = round_up(off, 16);
     return static_cast<std::size_t>(a.warp_bytes) * plan.warps_per_block;
 }

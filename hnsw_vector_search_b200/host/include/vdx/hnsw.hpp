@@ -29,6 +29,18 @@
 namespace vdx {
 
 struct DeviceGraph;  // vdx/device.hpp
+namespace dev {
+struct DeviceStopNet;
+}
+
+// The learned early-termination model (12 -> 64 -> 64 -> 1): 5,057 FP32 parameters, the
+// feature standardization, and the 4 random projection directions (4 rows of dim floats).
+struct StopModel {
+    std::vector<float> weights;
+    std::vector<float> mean;
+    std::vector<float> inv_std;
+    std::vector<float> proj;
+};
 
 struct HnswParams {
     std::size_t M = 16;                            // links per node per layer; 2M on layer 0
@@ -116,6 +128,20 @@ public:
     // Never uploads, so it never allocates.
     const DeviceGraph* uploaded_graph(int device, Precision precision) const;
 
+    // Learned early termination: the model SearchOptions::learned_stop uses.
+    void set_stop_model(StopModel model);
+    bool has_stop_model() const noexcept { return !stop_model_.weights.empty(); }
+    const StopModel& stop_model() const noexcept { return stop_model_; }
+
+    // Training traces: the plain search of every query at `ef`; every 8 expansions the 12
+    // features of its state (projections from `proj`, 4 rows of dim floats) and how many of its
+    // current top k are in `truth` (truth_k ids per query), and at the end the final hits.
+    // Buffers: features [nq][max_points][12], hits [nq][max_points], points [nq], final [nq].
+    void trace_search(MatrixView<float> queries, const Id* truth, std::size_t truth_k,
+                      std::size_t k, std::size_t ef, const float* proj, std::size_t max_points,
+                      float* features, std::uint8_t* hits, std::uint32_t* points,
+                      std::uint8_t* final_hits, int device = 0) const;
+
     // Read-only views of the graph, in the reference's in-memory layout.
     std::span<const std::uint8_t> levels() const noexcept { return levels_; }
     std::span<const Id> layer0() const noexcept { return layer0_; }
@@ -170,6 +196,8 @@ private:
     std::unique_ptr<BuildLocks> build_locks_;
     mutable std::unique_ptr<std::mutex> device_mutex_;
     mutable std::vector<std::unique_ptr<DeviceGraph>> device_;  // per (device, precision) slot
+    StopModel stop_model_;
+    mutable std::vector<std::shared_ptr<dev::DeviceStopNet>> stop_net_;  // per device
 };
 
 }  // namespace vdx

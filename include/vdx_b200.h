@@ -153,6 +153,36 @@ VDX_API vdx_status vdx_search_batch_device_noalloc(const vdx_index* index, const
                                                    uint32_t* d_counts,
                                                    const vdx_search_options* opts, void* stream);
 
+/* --- Learned early termination (no counterpart in the reference; its training and the
+ * in-search network are this library's own) ------------------------------------------------ */
+
+enum { VDX_STOP_PARAMS = 5057, VDX_STOP_FEATURES = 12 };
+
+/* The model vdx_search_options.learned_stop uses: weights[5057] (W1 64x12, b1, W2 64x64, b2, W3,
+ * b3), mean[12], inv_std[12], proj[4 x dim]. */
+VDX_API vdx_status vdx_index_set_stop_model(vdx_index* index, const float* weights,
+                                            const float* mean, const float* inv_std,
+                                            const float* proj);
+/* Training traces of the plain search at `ef` (see HnswIndex::trace_search): truth nq x
+ * truth_k ids; features nq x max_points x 12; hits nq x max_points; points, final_hits nq. */
+VDX_API vdx_status vdx_stop_trace(const vdx_index* index, const float* queries, uint64_t nq,
+                                  uint64_t dim, const uint32_t* truth, uint64_t truth_k,
+                                  uint64_t k, uint64_t ef, const float* proj, uint64_t max_points,
+                                  float* features, uint8_t* hits, uint32_t* points,
+                                  uint8_t* final_hits, int32_t device);
+/* Trains the network on the GPU (own forward, backward and Adam kernels) on raw features
+ * x[n][12] and labels y[n] in {0, 1}. Outputs weights[5057], mean[12], inv_std[12],
+ * loss_per_epoch[epochs]. */
+VDX_API vdx_status vdx_mlp_train(const float* x, const float* y, uint64_t n, uint32_t epochs,
+                                 uint64_t batch, float lr, uint64_t seed, float* weights,
+                                 float* mean, float* inv_std, float* loss_per_epoch);
+/* One GPU forward + backward over standardized x: grad[5057] of the mean loss, and the loss. */
+VDX_API vdx_status vdx_mlp_gradient(const float* x, const float* y, uint64_t n,
+                                    const float* weights, float* grad, float* loss);
+/* P(converged) for raw features x[n][12]. */
+VDX_API vdx_status vdx_mlp_probabilities(const float* x, uint64_t n, const float* weights,
+                                         const float* mean, const float* inv_std, float* prob);
+
 /* --- BruteForceIndex ----------------------------------------------------------------------- */
 
 /* BruteForceIndex(dim, metric): include/vecdex/brute_force.hpp:28 */
