@@ -39,7 +39,8 @@ N_BASE = 1_000_000
 N_QUERIES = 10_000
 K = 10
 M, EF_CONSTRUCTION, SEED = 16, 200, 42
-EF_SWEEP = [16, 24, 32, 48, 64, 96, 128, 192, 256, 384, 512]
+EF_SWEEP = [16, 20, 24, 28, 32, 36, 40, 44, 48, 56, 64, 80, 96, 128, 192, 256, 384, 512]
+TRAIN_QUERIES, CAL_QUERIES = 50_000, 5_000
 TARGET_RECALL = 0.95
 METRIC = "QPS at recall@10>=0.95, 1Mx128 L2, 1xB200: learned/BF16 vs plain GPU HNSW"
 
@@ -300,12 +301,16 @@ def main():
     modes = [("fp32", {}), ("bf16", {"precision": "bf16", "rerank": 40})]
     for _, o in modes:
         ix.upload(local, o.get("precision", "fp32"))
+    learned_info = learned_mode(v, ix, base, graph, local)
+    modes.append(("learned_bf16", {"precision": "bf16", "rerank": 40, "learned_stop": True,
+                                   "stop_threshold": learned_info["threshold"]}))
 
     # Operating points: the smallest swept ef reaching recall 0.95, per mode.
     points = {}
     sweep = {}
     for name, o in modes:
-        for ef in EF_SWEEP:
+        efs = [learned_info["ef_cap"]] if name == "learned_bf16" else EF_SWEEP
+        for ef in efs:
             ids, _, _ = ix.search_batch(queries, K, ef, device=local, **o)
             rec = recall_at_10(ids, truth)
             sweep.setdefault(name, []).append({"ef": ef, "recall": round(rec, 4)})
@@ -409,6 +414,8 @@ def main():
                        "parallelism": f"replicas x{world}"},
             "plain_fp32": {"qps": results["fp32"]["qps"], "ef": results["fp32"]["ef"],
                            "recall_at_10": round(results["fp32"]["recall"], 4)},
+            "speedup_vs_plain_fp32": r["qps"] / results["fp32"]["qps"],
+            "learned": learned_info,
             "modes": {n: {"qps": x["qps"], "ef": x["ef"], "recall_at_10": round(x["recall"], 4)}
                       for n, x in results.items()},
             "sweep": sweep,
@@ -428,6 +435,54 @@ def main():
     if pg is not None:
         pg.barrier()
         pg.destroy_process_group()
+
+
+def learned_mode(v, ix, base, graph, device) -> dict:
+    """Trains (or loads the cached) learned-termination model for this graph: traces of the
+    plain search at ef = 512 for 50,000 training queries (seed 21, the same mixture as the test
+    queries) judged by exact brute force, this library's training kernels, then the threshold
+    and ef cap calibrated on 5,000 more queries (seed 22) for recall@10 >= 0.955 with BF16
+    traversal. The 10,000 test queries are never used for training or calibration."""
+    from hnsw_vector_search_b200 import learned
+    from hnsw_vector_search_b200.datasets import integer_clusters
+    path = CACHE / (graph.stem + "_stop_model.npz")
+    info = {}
+    if path.exists():
+        model = learned.StopModel.load(path)
+        info["source"] = "cached"
+    else:
+        t0 = time.time()
+        bf = v.BruteForceIndex(base.shape[1], "l2")
+        bf.add(base)
+        train_q = integer_clusters(TRAIN_QUERIES, 128, 1000, seed=21, centers_seed=111)
+        cal_q = integer_clusters(CAL_QUERIES, 128, 1000, seed=22, centers_seed=111)
+        train_truth, _, _ = bf.search_batch(train_q, K, method="tensor_core")
+        cal_truth, _, _ = bf.search_batch(cal_q, K, method="tensor_core")
+        tr = learned.traces(ix, train_q, train_truth, k=K, ef=512, device=device)
+        x, y = learned.training_set(tr)
+        model, losses = learned.train(x, y, tr["proj"], epochs=6)
+        learned.attach(ix, model)
+        best = None
+        for cap in (48, 64, 96):
+            thr, rec = learned.calibrate(ix, model, cal_q, cal_truth, K, 0.955, cap,
+                                         precision="bf16", rerank=40, device=device)
+            ix.search_batch(cal_q, K, cap, precision="bf16", rerank=40, learned_stop=True,
+                            stop_threshold=thr, device=device)
+            work = v.HnswIndex.last_stats()["row_bytes"]
+            if rec >= 0.955 and (best is None or work < best[2]):
+                best = (thr, cap, work, rec)
+        if best is None:
+            best = (0.995, 96, 0, rec)
+        model.threshold, model.ef_cap = best[0], best[1]
+        model.save(path)
+        info.update({"source": "trained", "train_seconds": round(time.time() - t0, 1),
+                     "samples": int(len(x)), "positive_share": round(float(y.mean()), 3),
+                     "loss_first_last": [float(losses[0]), float(losses[-1])],
+                     "calibration_recall": round(best[3], 4)})
+    learned.attach(ix, model)
+    info.update({"threshold": model.threshold, "ef_cap": model.ef_cap,
+                 "train_queries": TRAIN_QUERIES, "calibration_queries": CAL_QUERIES})
+    return info
 
 
 def bruteforce_section(v, torch, base, queries, dev) -> dict:

@@ -274,6 +274,12 @@ vdx_status vdx_search_batch_device(const vdx_index* index, const float* d_querie
         a.stats = reinterpret_cast<unsigned long long*>(d_work + 16);
         const uint32_t kk = std::max<uint32_t>(k_uniform, 1);
         a.rerank = o.precision == vdx::Precision::FP32 ? 0U : (o.rerank > 0 ? o.rerank : 4 * kk);
+        if (o.learned_stop) {
+            const vdx::dev::DeviceStopNet& net = h.stop_net(o.device);
+            a.stop = net.view;
+            a.stop_enabled = &net;
+            a.stop_threshold = o.stop_threshold;
+        }
         // Per-query ef: the capacity must cover the largest; the caller's uniform ef bounds it.
         const uint64_t cap = std::min<uint64_t>(std::max<uint64_t>(ef_uniform, kk), h.size());
         const vdx::dev::SearchPlan plan = vdx::dev::default_plan(g.view, static_cast<uint32_t>(cap));

@@ -435,6 +435,13 @@ const dev::DeviceStopNet& stop_net_for(const HnswIndex& ix, std::mutex& m,
 
 }  // namespace
 
+const dev::DeviceStopNet& HnswIndex::stop_net(int device) const {
+    if (!device_mutex_) {
+        device_mutex_ = std::make_unique<std::mutex>();
+    }
+    return stop_net_for(*this, *device_mutex_, stop_net_, device, "HnswIndex::search_batch");
+}
+
 void HnswIndex::search_batch_into(MatrixView<float> queries, std::size_t k, std::size_t ef,
                                   Id* ids, float* distances, std::uint32_t* counts,
                                   const SearchOptions& options, const char* where) const {

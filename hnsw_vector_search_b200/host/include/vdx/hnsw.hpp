@@ -132,6 +132,8 @@ public:
     void set_stop_model(StopModel model);
     bool has_stop_model() const noexcept { return !stop_model_.weights.empty(); }
     const StopModel& stop_model() const noexcept { return stop_model_; }
+    // The model's device copy for `device`, uploaded on first use (throws without a model).
+    const dev::DeviceStopNet& stop_net(int device) const;
 
     // Training traces: the plain search of every query at `ef`; every 8 expansions the 12
     // features of its state (projections from `proj`, 4 rows of dim floats) and how many of its
