@@ -40,7 +40,7 @@ N_QUERIES = 10_000
 K = 10
 M, EF_CONSTRUCTION, SEED = 16, 200, 42
 EF_SWEEP = [16, 20, 24, 28, 32, 36, 40, 44, 48, 56, 64, 80, 96, 128, 192, 256, 384, 512]
-TRAIN_QUERIES, CAL_QUERIES = 50_000, 5_000
+TRAIN_QUERIES, CAL_QUERIES = 20_000, 5_000
 TARGET_RECALL = 0.95
 METRIC = "QPS at recall@10>=0.95, 1Mx128 L2, 1xB200: learned/BF16 vs plain GPU HNSW"
 
@@ -439,7 +439,7 @@ def main():
 
 def learned_mode(v, ix, base, graph, device) -> dict:
     """Trains (or loads the cached) learned-termination model for this graph: traces of the
-    plain search at ef = 512 for 50,000 training queries (seed 21, the same mixture as the test
+    plain search at ef = 512 for 20,000 training queries (seed 21, the same mixture as the test
     queries) judged by exact brute force, this library's training kernels, then the threshold
     and ef cap calibrated on 5,000 more queries (seed 22) for recall@10 >= 0.955 with BF16
     traversal. The 10,000 test queries are never used for training or calibration."""

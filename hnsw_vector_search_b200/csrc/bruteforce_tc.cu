@@ -142,6 +142,20 @@ __device__ __forceinline__ void tmem_ld32(std::uint32_t taddr, std::uint32_t (&r
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+// Order-preserving map of floats to u32 (so atomicMax on the key is max on the float).
+__device__ __forceinline__ std::uint32_t float_to_key(float f) {
+    const std::uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+// Keys below that of -inf (0x007FFFFF) would be NaNs and are never produced: the zeroed array
+// means "no floor yet" (-inf).
+__device__ __forceinline__ float key_to_float(std::uint32_t k) {
+    if (k < 0x007FFFFFu) {
+        return -INFINITY;
+    }
+    return __uint_as_float((k & 0x80000000u) ? (k & 0x7FFFFFFFu) : ~k);
+}
+
 // -------------------------------------------------------------------------------------------
 // Kernel parameters
 
@@ -154,6 +168,7 @@ struct TcParams {
     std::uint32_t* cand_ids;              // [nq][nchunks][kc]
     float* cand_d;
     float* cand_tau;                      // [nq][nchunks]
+    std::uint32_t* floor_key;             // [nq] best kc-th score of any finished chunk (ordered key)
     std::uint32_t* error;                 // status word: 5 on a timeout
     std::uint32_t off_b, off_lists, off_bar;  // smem offsets from the 1024-aligned base
 };
@@ -352,8 +367,11 @@ __global__ void __launch_bounds__(kThreads, 1)
             const std::uint32_t rows = min(p.chunk_rows, p.n - row0);
             const std::uint32_t tiles = (rows + kBN - 1) / kBN;
             std::uint32_t count = 0;
-            float thr = -INFINITY;  // the kc-th best score so far (-inf while the list is short)
-            std::uint32_t thr_i = kNoId;
+            // Scores at or below `floor` cannot reach the global best kc: another chunk already
+            // holds kc better ones (its list is part of the merge).
+            const float floor = live ? key_to_float(p.floor_key[row]) : INFINITY;
+            float thr = floor;          // acceptance bound: the floor, then the list's kc-th
+            std::uint32_t thr_i = kNoId;  // kNoId: ties with the bound are accepted
             bool ok = true;
             for (std::uint32_t t = 0; t < tiles; ++t, ++acc_it) {
                 const std::uint32_t b = acc_it & 1u;
@@ -373,7 +391,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                     const std::uint32_t id0 = row0 + t * kBN + cc * 32;
                     const float4* bias4 = reinterpret_cast<const float4*>(p.xnorm + id0);
                     float sc[32];
-                    float best = -INFINITY;
+                    std::uint32_t mask = 0;
 #pragma unroll
                     for (int q4 = 0; q4 < 8; ++q4) {
                         const float4 bv = __ldg(bias4 + q4);
@@ -383,21 +401,23 @@ __global__ void __launch_bounds__(kThreads, 1)
                             const float sv = __uint_as_float(r[4 * q4 + u]);
                             const float v = l2 ? __fmaf_rn(2.0F, sv, -bb[u]) : __fsub_rn(sv, bb[u]);
                             sc[4 * q4 + u] = v;
-                            best = fmaxf(best, v);
+                            mask |= (v >= thr ? 1u : 0u) << (4 * q4 + u);
                         }
                     }
-                    // Rows past the chunk end belong to the next chunk (never here: chunks are
-                    // whole tiles) or are padding (bias +inf, score -inf).
-                    if (!live || best < thr || (count == p.kc && best == thr && id0 > thr_i)) {
+                    if (!live) {
                         continue;
                     }
-#pragma unroll 1
-                    for (int j = 0; j < 32; ++j) {
-                        const float v = sc[j];
+                    // One iteration per candidate that may qualify; the bound only rises.
+                    while (mask != 0) {
+                        const int j = __ffs(mask) - 1;
+                        mask &= mask - 1;
+                        float v = sc[0];
+#pragma unroll
+                        for (int jj = 1; jj < 32; ++jj) {
+                            v = jj == j ? sc[jj] : v;
+                        }
                         const std::uint32_t id = id0 + static_cast<std::uint32_t>(j);
-                        const bool better = count < p.kc ? v > -INFINITY
-                                                         : (v > thr || (v == thr && id < thr_i));
-                        if (!better) {
+                        if (!(v > thr || (v == thr && id < thr_i))) {
                             continue;
                         }
                         std::uint32_t pos = count < p.kc ? count : p.kc - 1;
@@ -417,8 +437,12 @@ __global__ void __launch_bounds__(kThreads, 1)
                             ++count;
                         }
                         if (count == p.kc) {
-                            thr = list_d[(p.kc - 1) * kBM + e];
-                            thr_i = list_i[(p.kc - 1) * kBM + e];
+                            const float kth = list_d[(p.kc - 1) * kBM + e];
+                            const std::uint32_t kth_i = list_i[(p.kc - 1) * kBM + e];
+                            if (kth > thr || (kth == thr && thr_i == kNoId)) {
+                                thr = kth;
+                                thr_i = kth_i;
+                            }
                         }
                     }
                 }
@@ -435,8 +459,14 @@ __global__ void __launch_bounds__(kThreads, 1)
                     p.cand_d[at + i] = i < count ? (l2 ? __fsub_rn(qn, v) : __fsub_rn(1.0F, v)) : INFINITY;
                     p.cand_ids[at + i] = i < count ? list_i[i * kBM + e] : kNoId;
                 }
+                // Every excluded row of this chunk scored at most `thr` (the floor, or the full
+                // list's kc-th): no excluded distance is below the matching distance.
+                const float bound = count == p.kc ? fmaxf(thr, floor) : floor;
                 p.cand_tau[static_cast<std::size_t>(row) * p.nchunks + ch] =
-                    count == p.kc ? (l2 ? __fsub_rn(qn, thr) : __fsub_rn(1.0F, thr)) : INFINITY;
+                    bound == -INFINITY ? INFINITY : (l2 ? __fsub_rn(qn, bound) : __fsub_rn(1.0F, bound));
+                if (count == p.kc) {
+                    atomicMax(p.floor_key + row, float_to_key(list_d[(p.kc - 1) * kBM + e]));
+                }
             }
         }
     }
@@ -730,7 +760,7 @@ Plan make_plan(std::uint32_t nq, std::uint32_t n, std::uint32_t dim, std::uint32
     Plan pl{};
     pl.dk = static_cast<std::uint32_t>(align_up(dim, kBK));
     pl.kchunks = pl.dk / kBK;
-    pl.kc = k <= 16 ? 32 : (k <= 48 ? 64 : 0);
+    pl.kc = k <= 10 ? 16 : (k <= 24 ? 32 : (k <= 48 ? 64 : 0));
     pl.ok = pl.kc != 0 && pl.kchunks <= 4 && n >= 1;
     if (!pl.ok) {
         return pl;
@@ -854,7 +884,7 @@ std::size_t bruteforce_tc_workspace(std::uint32_t nq, std::uint32_t n, std::uint
            + 4 * nqp * row32                    // normalized FP32 queries
            + 4 * nqp * 3                        // norms, exact and valid flags
            + nq * chunks * kc * 8 + nq * chunks * 4  // candidates
-           + 4 * nqp + 4096 + 16 * 256;         // uncertified rows, flags, alignment
+           + 8 * nqp + 4096 + 16 * 256;         // uncertified rows, floors, flags, alignment
 }
 
 cudaError_t launch_bruteforce_tc(const BruteArgs& a, const TcBase& b, void* workspace,
@@ -888,9 +918,12 @@ cudaError_t launch_bruteforce_tc(const BruteArgs& a, const TcBase& b, void* work
     auto* cand_d = reinterpret_cast<float*>(take(static_cast<std::size_t>(nq) * pl.nchunks * pl.kc * 4));
     auto* cand_tau = reinterpret_cast<float*>(take(static_cast<std::size_t>(nq) * pl.nchunks * 4));
     auto* uncert = reinterpret_cast<std::uint32_t*>(take(nqp * 4));
+    auto* floor_key = reinterpret_cast<std::uint32_t*>(take(nqp * 4));
     auto* flags = reinterpret_cast<std::uint32_t*>(take(64));  // [0] query flags [1] max norm [2] error
 
     cudaError_t err = cudaMemsetAsync(flags, 0, 64, stream);
+    // Zero keys decode to -inf: no floor yet.
+    if (err == cudaSuccess) err = cudaMemsetAsync(floor_key, 0, nqp * 4, stream);
     if (err == cudaSuccess) err = cudaMemsetAsync(uncertified_out, 0, 4, stream);
     if (err == cudaSuccess && nqp > nq) {
         err = cudaMemsetAsync(q_hi + static_cast<std::size_t>(nq) * pl.dk, 0, (nqp - nq) * pl.dk * 2, stream);
@@ -940,6 +973,7 @@ cudaError_t launch_bruteforce_tc(const BruteArgs& a, const TcBase& b, void* work
     p.cand_ids = cand_ids;
     p.cand_d = cand_d;
     p.cand_tau = cand_tau;
+    p.floor_key = floor_key;
     p.error = a.status;
     p.off_b = pl.off_b;
     p.off_lists = pl.off_lists;
