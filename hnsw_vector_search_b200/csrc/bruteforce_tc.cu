@@ -648,9 +648,11 @@ __global__ void bf_tc_merge_kernel(const MergeParams p) {
     for (std::uint32_t ch = 0; ch < p.nchunks; ++ch) {
         const std::size_t at = (static_cast<std::size_t>(row) * p.nchunks + ch) * p.kc;
         for (std::uint32_t j0 = 0; j0 < p.kc; j0 += 32) {
-            const std::uint32_t id = p.cand_ids[at + j0 + lane];
-            const float d = p.cand_d[at + j0 + lane];
-            merge_round(rd, rid, r, static_cast<int>(p.kc), d, id, id != kNoId, ap, lane, unused);
+            // kc may be 16: lanes past this chunk's list read nothing.
+            const bool in = j0 + lane < p.kc;
+            const std::uint32_t id = in ? p.cand_ids[at + j0 + lane] : kNoId;
+            const float d = in ? p.cand_d[at + j0 + lane] : INFINITY;
+            merge_round(rd, rid, r, static_cast<int>(p.kc), d, id, id < p.n, ap, lane, unused);
         }
         tau = fminf(tau, p.cand_tau[static_cast<std::size_t>(row) * p.nchunks + ch]);
     }
