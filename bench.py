@@ -262,6 +262,9 @@ def main():
                     help="one search launch per warm-up step on the cached workload (for ncu)")
     ap.add_argument("--mode", default="fp32", choices=["fp32", "bf16", "fp8", "bf_tc", "bf_exact"])
     ap.add_argument("--ef", type=int, default=32)
+    ap.add_argument("--study", choices=["uneven", "precision"],
+                    help="instead of the headline: the uneven-batch stream or the precision study")
+    ap.add_argument("--rows", type=int, default=0, help="base rows of a study (0: its default)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank, world, local = dist_env()
@@ -287,6 +290,12 @@ def main():
     torch.cuda.set_device(local)
     if args.profile:
         profile(args, v, torch)
+        return
+    if args.study == "uneven":
+        study_uneven(args, v, torch)
+        return
+    if args.study == "precision":
+        study_precision(args, v, torch)
         return
     base, queries = workload()
     cpu = None
@@ -533,6 +542,189 @@ def bruteforce_section(v, torch, base, queries, dev) -> dict:
            "note": "pipeline time: query prep + tcgen05 GEMM/epilogue + merge/re-rank + exact "
                    "fallback for uncertified rows; the GEMM kernel's share is in profiles/"}
     return out
+
+
+def cached_graph(v, name: str, base, metric: str, m: int):
+    """An index over `base` built by this library's parallel host build, cached on disk."""
+    path = CACHE / f"{name}_M{m}_efc{EF_CONSTRUCTION}.vdx"
+    if path.exists():
+        return v.HnswIndex.load(path)
+    t = time.time()
+    ix = v.HnswIndex(base.shape[1], metric, M=m, ef_construction=EF_CONSTRUCTION, seed=SEED)
+    ix.add(base, num_threads=0)
+    ix.save(path)
+    log(f"{name}: built in {time.time() - t:.1f} s on {os.cpu_count()} threads")
+    return ix
+
+
+def request_stream(n_requests: int, seed: int):
+    """(size, k, ef) per request: size log-uniform in [1, 4096], k in {1, 10, 100}, ef uniform
+    in [k, 4k + 256]."""
+    g = np.random.Generator(np.random.PCG64(seed))
+    sizes = np.floor(np.exp(g.uniform(0.0, np.log(4097.0), size=n_requests))).astype(np.int64)
+    sizes = np.clip(sizes, 1, 4096)
+    ks = g.choice(np.array([1, 10, 100]), size=n_requests)
+    efs = np.array([g.integers(k, 4 * k + 257) for k in ks])
+    return sizes, ks, efs
+
+
+def study_uneven(args, v, torch):
+    """The uneven-batch stream: 5,000 requests (seed 51) of log-uniform size in [1, 4096],
+    k in {1, 10, 100} and ef in [k, 4k + 256] over an inner-product index of 96-d vectors in
+    4,096 clusters with log-normal scales (M = 24, ef_construction = 200). Three ways to serve
+    it, all through host buffers (copies in the timed region), closed loop:
+      per_request  HnswIndex.search_batch per request (the plain batch API);
+      batcher      one captured-graph replay per request (ef classes, autotuned plans);
+      packed       consecutive requests packed into batches of <= 4096 queries, one replay each.
+    Reported: queries/s over the stream and per-request latency (p50 / p99, from the start of the
+    call that serves the request to its results on the host). Every request's rows are checked
+    against the plain search on a sample."""
+    from hnsw_vector_search_b200.datasets import scaled_clusters
+    n = args.rows or 1_000_000
+    CACHE.mkdir(exist_ok=True)
+    f = CACHE / f"scaled_ip_{n}.npz"
+    if f.exists():
+        z = np.load(f)
+        base, pool = z["base"], z["pool"]
+    else:
+        base = scaled_clusters(n, 96, 4096, seed=51, centers_seed=151)
+        pool = scaled_clusters(50_000, 96, 4096, seed=52, centers_seed=151)
+        np.savez(f, base=base, pool=pool)
+    ix = cached_graph(v, f"scaled_ip_{n}", base, "ip", 24)
+    ix.upload(0, "fp32")
+    sizes, ks, efs = request_stream(5000, 51)
+    offs = np.concatenate([[0], np.cumsum(sizes)])
+    rows = np.arange(offs[-1]) % len(pool)
+    requests = [(pool[rows[offs[i]:offs[i + 1]]], int(ks[i]), int(efs[i])) for i in range(len(sizes))]
+    total_q = int(offs[-1])
+    log(f"uneven stream: {len(requests)} requests, {total_q} queries")
+
+    bt = v.Batcher(ix, max_queries=4096, max_k=100, max_ef=4 * 100 + 256)
+
+    def pack(reqs):
+        batches, cur, cur_n = [], [], 0
+        for i, (q, _, _) in enumerate(reqs):
+            if cur and cur_n + len(q) > 4096:
+                batches.append(cur)
+                cur, cur_n = [], 0
+            cur.append(i)
+            cur_n += len(q)
+        if cur:
+            batches.append(cur)
+        return batches
+
+    batches = pack(requests)
+    sample = batches[len(batches) // 2]
+    sq = np.concatenate([requests[i][0] for i in sample])
+    sk = np.concatenate([np.full(len(requests[i][0]), requests[i][1], np.uint32) for i in sample])
+    se = np.concatenate([np.full(len(requests[i][0]), requests[i][2], np.uint32) for i in sample])
+    t0 = time.time()
+    tuned = bt.autotune(sq, sk, se)
+    tune_s = time.time() - t0
+    chosen = {}
+    for t in tuned:
+        c = chosen.get(t["ef_class"])
+        if c is None or t["ms"] < c["ms"]:
+            chosen[t["ef_class"]] = t
+
+    # Parity on every 50th request: the batcher's rows equal the plain search's.
+    mismatches = 0
+    for i in range(0, len(requests), 50):
+        q, k, ef = requests[i]
+        a, b, c = bt.run(q, k, ef)
+        wa, wb, wc = ix.search_batch(q, k, ef)
+        if not (np.array_equal(a[:, :k], wa) and np.array_equal(b[:, :k], wb) and np.array_equal(c, wc)):
+            mismatches += 1
+
+    def serve(mode):
+        lat = np.zeros(len(requests))
+        torch.cuda.synchronize()
+        t_all = time.perf_counter()
+        if mode == "packed":
+            for b in batches:
+                t0 = time.perf_counter()
+                q = np.concatenate([requests[i][0] for i in b])
+                kk = np.concatenate([np.full(len(requests[i][0]), requests[i][1], np.uint32) for i in b])
+                ee = np.concatenate([np.full(len(requests[i][0]), requests[i][2], np.uint32) for i in b])
+                bt.run(q, kk, ee)
+                lat[b] = time.perf_counter() - t0
+        else:
+            for i, (q, k, ef) in enumerate(requests):
+                t0 = time.perf_counter()
+                if mode == "batcher":
+                    bt.run(q, k, ef)
+                else:
+                    ix.search_batch(q, k, ef)
+                lat[i] = time.perf_counter() - t0
+        wall = time.perf_counter() - t_all
+        return {"queries_per_s": total_q / wall, "seconds": wall,
+                "latency_ms_p50": float(np.percentile(lat, 50) * 1e3),
+                "latency_ms_p99": float(np.percentile(lat, 99) * 1e3)}
+
+    out = {}
+    with Clocks(0) as clocks:
+        for mode in ("per_request", "batcher", "packed"):
+            serve(mode)  # warm-up pass
+            out[mode] = serve(mode)
+    line = {"study": "uneven", "workload": f"{n} x 96 IP, 4,096 clusters (log-normal scales), "
+                                           f"M24 efc{EF_CONSTRUCTION}; 5,000 requests (seed 51)",
+            "queries": total_q, "batches_packed": len(batches), "modes": out,
+            "autotune_seconds": round(tune_s, 2),
+            "plans": {str(k_): {f: c[f] for f in ("warps_per_block", "rows_per_round", "hash_slots",
+                                                   "result_capacity", "ms")}
+                      for k_, c in sorted(chosen.items())},
+            "parity_sampled_requests": len(range(0, len(requests), 50)),
+            "parity_mismatches": mismatches, "clocks": clocks.summary()}
+    print(json.dumps(line), flush=True)
+
+
+def study_precision(args, v, torch):
+    """Precision study on the GloVe-like cosine workload (1,183,514 x 100, Student-t(3)
+    coordinates through a seeded mixing matrix, unit rows; 10,000 queries, 2% duplicates of base
+    rows): per ef and traversal precision (FP32; BF16 and FP8-E4M3 with an FP32 re-rank of the
+    best 4k = 40, and without re-rank), recall@10 against exact brute force and the max / mean
+    absolute error of the returned distances against FP64 distances of the same ids."""
+    from hnsw_vector_search_b200.datasets import config_glove_like
+    n = args.rows or 1_183_514
+    CACHE.mkdir(exist_ok=True)
+    f = CACHE / f"glove_like_{n}.npz"
+    if f.exists():
+        z = np.load(f)
+        base, queries = z["base"], z["queries"]
+    else:
+        base, queries = config_glove_like(n, N_QUERIES)
+        np.savez(f, base=base, queries=queries)
+    ix = cached_graph(v, f"glove_like_{n}", base, "cosine", 16)
+    bf = v.BruteForceIndex(base.shape[1], "cosine")
+    bf.add(base)
+    truth, _, _ = bf.search_batch(queries, K)
+    # FP64 judge: the stored (normalized) rows against the FP64-normalized query.
+    q64 = queries.astype(np.float64)
+    q64 /= np.linalg.norm(q64, axis=1, keepdims=True)
+    stored = base.astype(np.float64)
+    stored /= np.linalg.norm(stored, axis=1, keepdims=True)
+    stored = stored.astype(np.float32).astype(np.float64)
+
+    def errors(ids, d):
+        valid = ids != 0xFFFFFFFF
+        rows = np.where(valid, ids, 0).astype(np.int64)
+        d64 = 1.0 - np.einsum("qd,qkd->qk", q64, stored[rows])
+        e = np.abs(d.astype(np.float64) - d64)[valid]
+        return float(e.max()), float(e.mean())
+
+    modes = [("fp32", {}), ("bf16+rerank40", {"precision": "bf16", "rerank": 40}),
+             ("fp8+rerank40", {"precision": "fp8", "rerank": 40}),
+             ("bf16", {"precision": "bf16", "rerank": 0}), ("fp8", {"precision": "fp8", "rerank": 0})]
+    table = {}
+    for name, o in modes:
+        for ef in (16, 32, 64, 128, 256, 512):
+            ids, d, _ = ix.search_batch(queries, K, ef, **o)
+            mx, mean = errors(ids, d)
+            table.setdefault(name, []).append({"ef": ef, "recall_at_10": round(recall_at_10(ids, truth), 4),
+                                               "max_abs_err": mx, "mean_abs_err": mean})
+    print(json.dumps({"study": "precision", "workload": f"{n} x 100 cosine glove-like, "
+                      f"10k queries (2% duplicates), M16 efc{EF_CONSTRUCTION}", "k": K,
+                      "table": table}), flush=True)
 
 
 def profile(args, v, torch):

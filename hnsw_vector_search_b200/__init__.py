@@ -38,6 +38,11 @@ class _IndexInfo(ctypes.Structure):
                 ("memory_bytes", _U64), ("metric", _U32)]
 
 
+class _PlanTiming(ctypes.Structure):
+    _fields_ = [("ef_class", _U32), ("warps_per_block", _I32), ("rows_per_round", _U32), ("hash_slots", _U32),
+                ("result_capacity", _U32), ("ms", _F)]
+
+
 class _GraphReport(ctypes.Structure):
     _fields_ = [("violations", _U64), ("reachable", _U64), ("max_level", _U64),
                 ("mean_degree0", ctypes.c_double)]
@@ -88,6 +93,10 @@ def lib() -> ctypes.CDLL:
         "vdx_bf_search_batch": (ctypes.c_int, [_P, _P, _U64, _U64, _U64, _U32, _P, _P, _P]),
         "vdx_bf_search_batch_device": (ctypes.c_int, [_P, _P, _U64, _U64, _U64, _U32, _P, _P, _P,
                                                       _P, _P]),
+        "vdx_batcher_create": (ctypes.c_int, [_P, _I32, _U32, _U32, _U32, _U32, ctypes.POINTER(_P)]),
+        "vdx_batcher_free": (None, [_P]),
+        "vdx_batcher_run": (ctypes.c_int, [_P, _P, _U64, _P, _P, _P, _P, _P]),
+        "vdx_batcher_autotune": (ctypes.c_int, [_P, _P, _U64, _P, _P, _P, _U64, ctypes.POINTER(_U64)]),
         "vdx_host_l2": (_F, [_P, _P, _U64]),
         "vdx_host_ip": (_F, [_P, _P, _U64]),
         "vdx_xxh64": (_U64, [_P, _U64, _U64]),
@@ -245,6 +254,58 @@ class HnswIndex:
             self._h, p(queries), nq, queries.shape[1], p(k_per_query), p(ef_per_query),
             k_uniform, ef_uniform, out_stride, p(ids), p(dists), p(counts), p(work),
             ctypes.byref(opts), stream))
+
+
+class Batcher:
+    """Uneven batches (any size up to max_queries, per-query k and ef) through one CUDA graph
+    captured at construction and replayed per batch. Queries are split into ef classes
+    (effective ef <= 64, <= 256, <= 1024, ...) that run as concurrent graph branches, each with
+    its own launch plan; `autotune` picks those plans. Row i of a result equals
+    HnswIndex.search_batch of query i with its own k and ef.
+
+    The batcher keeps the device graph it was made with: make a new one after adding vectors."""
+
+    def __init__(self, index: HnswIndex, max_queries: int, max_k: int, max_ef: int,
+                 precision: str = "fp32", device: int = 0):
+        self.index = index
+        self.max_k = int(max_k)
+        h = _P()
+        _raise(lib().vdx_batcher_create(index.handle, device, PRECISIONS[precision], max_queries,
+                                        max_k, max_ef, ctypes.byref(h)))
+        self._h = h.value
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().vdx_batcher_free(self._h)
+            self._h = None
+
+    @staticmethod
+    def _per_query(v, nq):
+        return np.ascontiguousarray(np.broadcast_to(np.asarray(v, np.uint32), (nq,)))
+
+    def run(self, queries, k, ef):
+        """(ids [nq, max_k], distances [nq, max_k], counts [nq]); row i holds k[i] results."""
+        q = _rows(queries, self.index.dim)
+        nq = q.shape[0]
+        kk, ee = self._per_query(k, nq), self._per_query(ef, nq)
+        ids = np.empty((nq, self.max_k), np.uint32)
+        d = np.empty((nq, self.max_k), np.float32)
+        c = np.empty(nq, np.uint32)
+        _raise(lib().vdx_batcher_run(self._h, _ptr(q), nq, _ptr(kk), _ptr(ee), _ptr(ids), _ptr(d),
+                                     _ptr(c)))
+        return ids, d, c
+
+    def autotune(self, queries, k, ef) -> list[dict]:
+        """Times every candidate plan on this batch and keeps the fastest; returns the timings."""
+        q = _rows(queries, self.index.dim)
+        nq = q.shape[0]
+        kk, ee = self._per_query(k, nq), self._per_query(ef, nq)
+        out = (_PlanTiming * 64)()
+        n = _U64()
+        _raise(lib().vdx_batcher_autotune(self._h, _ptr(q), nq, _ptr(kk), _ptr(ee),
+                                          ctypes.addressof(out), 64, ctypes.byref(n)))
+        return [{f: getattr(out[i], f) for f, _ in _PlanTiming._fields_}
+                for i in range(min(n.value, 64))]
 
 
 class BruteForceIndex:

@@ -1,0 +1,357 @@
+// Uneven batches through one captured launch graph.
+//
+// A request stream mixes batch sizes (1 .. thousands of queries), k and ef. The search kernel
+// already reads each query's k and ef, and the batch size, from device memory, so one captured
+// launch serves any batch up to a fixed capacity. What a single launch cannot do well is mix a
+// query at ef = 600 with queries at ef = 20: its shared-memory plan (result-list capacity,
+// visited-filter slots) is sized for the largest ef, which cuts the resident warps for every
+// query. So the Batcher splits each batch into ef classes (effective ef <= 64, <= 256, <= 1024,
+// ... up to the largest ef it accepts), each with its own plan and fixed device / pinned
+// buffers. The graph holds one branch per class (work-word reset + persistent search kernel);
+// the branches run concurrently, so one class's blocks fill the SMs another class's tail
+// leaves idle. Within a class the rows are staged longest-first (descending ef), the classic
+// longest-processing-time order, so the persistent warps that claim rows in order finish
+// together.
+//
+// Per batch the host stages the rows (pinned), issues one copy per class buffer, replays the
+// graph and copies the results back; results return in the caller's row order. The autotuner
+// times candidate plans (warps per block, rows per gather round, visited-filter slots) for each
+// class on a sample batch with CUDA events and keeps each class's fastest.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <format>
+#include <numeric>
+#include <stdexcept>
+#include <vector>
+
+#include "batcher.cuh"
+#include "gpu_runtime.cuh"
+#include "search.cuh"
+#include "vdx/device.hpp"
+
+namespace vdx::dev {
+
+namespace {
+
+template <typename T>
+T* dalloc(std::size_t n, const char* what) {
+    void* p = gpu::device_alloc(std::max<std::size_t>(n, 1) * sizeof(T), what);
+    gpu::check(cudaMemset(p, 0, std::max<std::size_t>(n, 1) * sizeof(T)), what);
+    return static_cast<T*>(p);
+}
+template <typename T>
+T* halloc(std::size_t n) {
+    void* p = nullptr;
+    gpu::check(cudaMallocHost(&p, std::max<std::size_t>(n, 1) * sizeof(T)), "cudaMallocHost");
+    std::memset(p, 0, std::max<std::size_t>(n, 1) * sizeof(T));
+    return static_cast<T*>(p);
+}
+
+constexpr std::uint32_t kWorkWords = 64;
+constexpr std::uint32_t kRerankPerK = 4;
+
+}  // namespace
+
+Batcher::Batcher(const HnswIndex& idx, int dev, Precision prec, std::uint32_t max_q,
+                 std::uint32_t max_k_, std::uint32_t max_ef_)
+    : index(idx), device(dev), precision(prec), max_queries(max_q), max_k(max_k_), max_ef(max_ef_) {
+    if (max_q == 0 || max_k_ == 0) {
+        throw std::invalid_argument("Batcher: max_queries and max_k must be positive");
+    }
+    if (index.size() == 0) {
+        throw std::invalid_argument("Batcher: the index is empty");
+    }
+    gpu::use_device(device);
+    index_size = index.size();
+    graph_view = index.device_graph(device, precision).view;
+    dim = static_cast<std::uint32_t>(index.dim());
+    gpu::check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "stream");
+    gpu::check(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming), "event");
+
+    const std::uint32_t n = static_cast<std::uint32_t>(std::min<std::size_t>(index_size, 0xFFFFFFFFu));
+    const std::uint32_t top = std::max<std::uint32_t>(1, std::min(std::max(max_ef, max_k), n));
+    std::vector<std::uint32_t> caps;
+    for (std::uint32_t c = 64; c < top; c *= 4) {
+        caps.push_back(c);
+    }
+    caps.push_back(top);
+    classes.resize(caps.size());
+    joins.resize(caps.size());
+    const std::size_t rows_q = static_cast<std::size_t>(max_q) * dim;
+    const std::size_t rows_out = static_cast<std::size_t>(max_q) * max_k;
+    for (std::size_t i = 0; i < caps.size(); ++i) {
+        EfClass& c = classes[i];
+        c.cap = caps[i];
+        c.plan = default_plan(graph_view, c.cap);
+        gpu::check(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking), "stream");
+        gpu::check(cudaEventCreateWithFlags(&joins[i], cudaEventDisableTiming), "event");
+        c.d_queries = dalloc<float>(rows_q, "batch queries");
+        c.d_k = dalloc<std::uint32_t>(max_q, "batch k");
+        c.d_ef = dalloc<std::uint32_t>(max_q, "batch ef");
+        c.d_nq = dalloc<std::uint32_t>(1, "batch size");
+        c.d_ids = dalloc<std::uint32_t>(rows_out, "batch ids");
+        c.d_dists = dalloc<float>(rows_out, "batch distances");
+        c.d_counts = dalloc<std::uint32_t>(max_q, "batch counts");
+        c.d_work = dalloc<std::uint32_t>(kWorkWords, "batch work words");
+        c.h_queries = halloc<float>(rows_q);
+        c.h_k = halloc<std::uint32_t>(max_q);
+        c.h_ef = halloc<std::uint32_t>(max_q);
+        c.h_nq = halloc<std::uint32_t>(1);
+        c.h_ids = halloc<std::uint32_t>(rows_out);
+        c.h_dists = halloc<float>(rows_out);
+        c.h_counts = halloc<std::uint32_t>(max_q);
+        c.h_work = halloc<std::uint32_t>(kWorkWords);
+    }
+    capture();
+}
+
+Batcher::~Batcher() {
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(device);
+    if (stream != nullptr) {
+        cudaStreamSynchronize(stream);
+    }
+    if (exec != nullptr) {
+        cudaGraphExecDestroy(exec);
+    }
+    if (graph != nullptr) {
+        cudaGraphDestroy(graph);
+    }
+    for (EfClass& c : classes) {
+        if (c.stream != nullptr) {
+            cudaStreamSynchronize(c.stream);
+            cudaStreamDestroy(c.stream);
+        }
+        for (void* p : {static_cast<void*>(c.d_queries), static_cast<void*>(c.d_k),
+                        static_cast<void*>(c.d_ef), static_cast<void*>(c.d_nq),
+                        static_cast<void*>(c.d_ids), static_cast<void*>(c.d_dists),
+                        static_cast<void*>(c.d_counts), static_cast<void*>(c.d_work)}) {
+            cudaFree(p);
+        }
+        for (void* p : {static_cast<void*>(c.h_queries), static_cast<void*>(c.h_k),
+                        static_cast<void*>(c.h_ef), static_cast<void*>(c.h_nq),
+                        static_cast<void*>(c.h_ids), static_cast<void*>(c.h_dists),
+                        static_cast<void*>(c.h_counts), static_cast<void*>(c.h_work)}) {
+            cudaFreeHost(p);
+        }
+    }
+    for (cudaEvent_t e : joins) {
+        if (e != nullptr) {
+            cudaEventDestroy(e);
+        }
+    }
+    if (fork != nullptr) {
+        cudaEventDestroy(fork);
+    }
+    if (stream != nullptr) {
+        cudaStreamDestroy(stream);
+    }
+    cudaSetDevice(prev);
+}
+
+SearchArgs Batcher::args(const EfClass& c) const {
+    SearchArgs a;
+    a.g = graph_view;
+    a.queries = c.d_queries;
+    a.nq = max_queries;   // capacity; the batch size is read from d_nq
+    a.qstride = dim;
+    a.nq_device = c.d_nq;
+    a.k_per_q = c.d_k;
+    a.ef_per_q = c.d_ef;
+    a.k = max_k;
+    a.ef = c.cap;
+    a.out_stride = max_k;
+    a.out_ids = c.d_ids;
+    a.out_dists = c.d_dists;
+    a.out_counts = c.d_counts;
+    a.status = c.d_work;
+    a.claim = c.d_work + 2;
+    a.stats = reinterpret_cast<unsigned long long*>(c.d_work + 16);
+    if (precision != Precision::FP32) {
+        // As the batch search: an FP32 re-rank of the best 4 * k of each query.
+        a.rerank = kRerankPerK * max_k;
+        a.rerank_per_k = kRerankPerK;
+    }
+    return a;
+}
+
+void Batcher::enqueue(const EfClass& c, const SearchPlan& p, cudaStream_t s) {
+    gpu::check(cudaMemsetAsync(c.d_work, 0, kWorkWords * 4, s), "reset work words");
+    gpu::check(cudaMemsetAsync(c.d_work + 1, 0xFF, 4, s), "reset work words");
+    SearchArgs a = args(c);
+    gpu::check(launch_search(a, p, s), "search kernel");
+}
+
+void Batcher::capture() {
+    gpu::use_device(device);
+    if (exec != nullptr) {
+        cudaGraphExecDestroy(exec);
+        exec = nullptr;
+    }
+    if (graph != nullptr) {
+        cudaGraphDestroy(graph);
+        graph = nullptr;
+    }
+    gpu::check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+    gpu::check(cudaEventRecord(fork, stream), "fork");
+    for (std::size_t i = 0; i < classes.size(); ++i) {
+        gpu::check(cudaStreamWaitEvent(classes[i].stream, fork, 0), "fork");
+        enqueue(classes[i], classes[i].plan, classes[i].stream);
+        gpu::check(cudaEventRecord(joins[i], classes[i].stream), "join");
+        gpu::check(cudaStreamWaitEvent(stream, joins[i], 0), "join");
+    }
+    gpu::check(cudaStreamEndCapture(stream, &graph), "end capture");
+    gpu::check(cudaGraphInstantiate(&exec, graph, 0), "instantiate graph");
+}
+
+void Batcher::stage(const float* queries, std::uint32_t nq, const std::uint32_t* k,
+                    const std::uint32_t* ef) {
+    if (index.size() != index_size) {
+        throw std::invalid_argument("Batcher: the index changed since the batcher was made");
+    }
+    if (nq > max_queries) {
+        throw std::invalid_argument(std::format("Batcher: batch of {} exceeds the maximum {}", nq, max_queries));
+    }
+    for (EfClass& c : classes) {
+        c.rows.clear();
+    }
+    const std::uint32_t n = classes.back().cap;  // min(max(max_ef, max_k), size)
+    std::vector<std::uint32_t> eff(nq);
+    for (std::uint32_t i = 0; i < nq; ++i) {
+        if (k[i] == 0 || k[i] > max_k) {
+            throw std::invalid_argument(std::format("Batcher: k {} outside [1, {}]", k[i], max_k));
+        }
+        std::uint64_t e = std::max(ef[i], k[i]);
+        if (e > max_ef && e < index_size) {
+            throw std::invalid_argument(std::format("Batcher: ef {} above the maximum {}", ef[i], max_ef));
+        }
+        // ef >= size searches exhaustively; every such query behaves alike.
+        eff[i] = static_cast<std::uint32_t>(std::min<std::uint64_t>(e, std::min<std::uint64_t>(index_size, n)));
+        std::size_t ci = 0;
+        while (classes[ci].cap < eff[i]) {
+            ++ci;
+        }
+        classes[ci].rows.push_back(i);
+    }
+    for (EfClass& c : classes) {
+        std::stable_sort(c.rows.begin(), c.rows.end(),
+                         [&](std::uint32_t x, std::uint32_t y) { return eff[x] > eff[y]; });
+        const std::uint32_t m = static_cast<std::uint32_t>(c.rows.size());
+        for (std::uint32_t j = 0; j < m; ++j) {
+            const std::uint32_t i = c.rows[j];
+            std::memcpy(c.h_queries + static_cast<std::size_t>(j) * dim,
+                        queries + static_cast<std::size_t>(i) * dim, dim * 4ull);
+            c.h_k[j] = k[i];
+            c.h_ef[j] = ef[i];
+        }
+        *c.h_nq = m;
+        if (m > 0) {
+            gpu::check(cudaMemcpyAsync(c.d_queries, c.h_queries, static_cast<std::size_t>(m) * dim * 4,
+                                       cudaMemcpyHostToDevice, stream), "copy queries");
+            gpu::check(cudaMemcpyAsync(c.d_k, c.h_k, m * 4ull, cudaMemcpyHostToDevice, stream), "copy k");
+            gpu::check(cudaMemcpyAsync(c.d_ef, c.h_ef, m * 4ull, cudaMemcpyHostToDevice, stream), "copy ef");
+        }
+        gpu::check(cudaMemcpyAsync(c.d_nq, c.h_nq, 4, cudaMemcpyHostToDevice, stream), "copy batch size");
+    }
+}
+
+void Batcher::run(const float* queries, std::uint32_t nq, const std::uint32_t* k,
+                  const std::uint32_t* ef, std::uint32_t* ids, float* dists,
+                  std::uint32_t* counts) {
+    gpu::use_device(device);
+    stage(queries, nq, k, ef);
+    gpu::check(cudaGraphLaunch(exec, stream), "graph launch");
+    for (EfClass& c : classes) {
+        const std::size_t m = c.rows.size();
+        if (m > 0) {
+            gpu::check(cudaMemcpyAsync(c.h_ids, c.d_ids, m * max_k * 4, cudaMemcpyDeviceToHost, stream),
+                       "copy ids");
+            gpu::check(cudaMemcpyAsync(c.h_dists, c.d_dists, m * max_k * 4, cudaMemcpyDeviceToHost, stream),
+                       "copy distances");
+            gpu::check(cudaMemcpyAsync(c.h_counts, c.d_counts, m * 4, cudaMemcpyDeviceToHost, stream),
+                       "copy counts");
+        }
+        gpu::check(cudaMemcpyAsync(c.h_work, c.d_work, kWorkWords * 4, cudaMemcpyDeviceToHost, stream),
+                   "copy status");
+    }
+    gpu::check(cudaStreamSynchronize(stream), "batch");
+    for (const EfClass& c : classes) {
+        gpu::raise_status(c.h_work[0], "Batcher::run");
+    }
+    for (const EfClass& c : classes) {
+        for (std::size_t j = 0; j < c.rows.size(); ++j) {
+            const std::size_t i = c.rows[j];
+            std::memcpy(ids + i * max_k, c.h_ids + j * max_k, max_k * 4ull);
+            std::memcpy(dists + i * max_k, c.h_dists + j * max_k, max_k * 4ull);
+            counts[i] = c.h_counts[j];
+        }
+    }
+}
+
+float Batcher::time_plan(const EfClass& c, const SearchPlan& p, int reps) {
+    cudaEvent_t a, b;
+    gpu::check(cudaEventCreate(&a), "event");
+    gpu::check(cudaEventCreate(&b), "event");
+    enqueue(c, p, stream);  // warm-up
+    gpu::check(cudaEventRecord(a, stream), "event");
+    for (int i = 0; i < reps; ++i) {
+        enqueue(c, p, stream);
+    }
+    gpu::check(cudaEventRecord(b, stream), "event");
+    gpu::check(cudaEventSynchronize(b), "event");
+    float ms = 0.0F;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    gpu::check(cudaMemcpy(c.h_work, c.d_work, kWorkWords * 4, cudaMemcpyDeviceToHost), "copy status");
+    gpu::raise_status(c.h_work[0], "Batcher::autotune");
+    return ms / static_cast<float>(reps);
+}
+
+std::vector<TunedPlan> Batcher::autotune(const float* queries, std::uint32_t nq,
+                                         const std::uint32_t* k, const std::uint32_t* ef) {
+    gpu::use_device(device);
+    stage(queries, nq, k, ef);
+    gpu::check(cudaStreamSynchronize(stream), "stage");
+    std::vector<TunedPlan> tried;
+    for (EfClass& c : classes) {
+        if (c.rows.empty()) {
+            continue;
+        }
+        const SearchPlan base = default_plan(graph_view, c.cap);
+        SearchPlan best = base;
+        float best_ms = -1.0F;
+        for (const int warps : {2, 4, 8}) {
+            for (const std::uint32_t rows : {8u, 16u, 32u}) {
+                for (const std::uint32_t slots : {base.hash_slots / 2, base.hash_slots, base.hash_slots * 2}) {
+                    if (slots < 512) {
+                        continue;
+                    }
+                    SearchPlan p = base;
+                    p.warps_per_block = warps;
+                    p.rows_cap = std::max<std::uint32_t>(1, std::min(rows, graph_view.cap0));
+                    p.hash_slots = slots;
+                    SearchArgs a = args(c);
+                    if (plan_search(a, p) > 200 * 1024) {
+                        continue;
+                    }
+                    const float ms = time_plan(c, p, 3);
+                    tried.push_back({c.cap, p, ms});
+                    if (best_ms < 0.0F || ms < best_ms) {
+                        best_ms = ms;
+                        best = p;
+                    }
+                }
+            }
+        }
+        c.plan = best;
+    }
+    capture();
+    return tried;
+}
+
+}  // namespace vdx::dev

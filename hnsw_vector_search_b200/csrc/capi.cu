@@ -13,6 +13,7 @@
 #include "../../include/vdx_b200.h"
 #include "../host/src/internal.hpp"
 #include "capi_internal.hpp"
+#include "batcher.cuh"
 #include "gpu_runtime.cuh"
 #include "mlp.cuh"
 #include "search.cuh"
@@ -284,6 +285,55 @@ vdx_status vdx_search_batch_device(const vdx_index* index, const float* d_querie
         const uint64_t cap = std::min<uint64_t>(std::max<uint64_t>(ef_uniform, kk), h.size());
         const vdx::dev::SearchPlan plan = vdx::dev::default_plan(g.view, static_cast<uint32_t>(cap));
         vdx::gpu::check(vdx::dev::launch_search(a, plan, s), "search kernel");
+    });
+}
+
+struct vdx_batcher {
+    vdx::dev::Batcher b;
+};
+
+vdx_status vdx_batcher_create(const vdx_index* index, int32_t device, uint32_t precision,
+                              uint32_t max_queries, uint32_t max_k, uint32_t max_ef,
+                              vdx_batcher** out) {
+    return guarded([&] {
+        require(index, "index");
+        require(out, "out");
+        if (precision > 2) {
+            throw std::invalid_argument("unknown precision");
+        }
+        *out = new vdx_batcher{vdx::dev::Batcher(index->index, device,
+                                                 static_cast<vdx::Precision>(precision), max_queries,
+                                                 max_k, max_ef)};
+    });
+}
+
+void vdx_batcher_free(vdx_batcher* batcher) { delete batcher; }
+
+vdx_status vdx_batcher_run(vdx_batcher* batcher, const float* queries, uint64_t nq,
+                           const uint32_t* k_per_q, const uint32_t* ef_per_q, uint32_t* ids,
+                           float* dists, uint32_t* counts) {
+    return guarded([&] {
+        require(batcher, "batcher");
+        if (nq == 0) {
+            return;
+        }
+        batcher->b.run(queries, static_cast<uint32_t>(nq), k_per_q, ef_per_q, ids, dists, counts);
+    });
+}
+
+vdx_status vdx_batcher_autotune(vdx_batcher* batcher, const float* queries, uint64_t nq,
+                                const uint32_t* k_per_q, const uint32_t* ef_per_q,
+                                vdx_plan_timing* timings, uint64_t cap, uint64_t* n_out) {
+    return guarded([&] {
+        require(batcher, "batcher");
+        const auto tried = batcher->b.autotune(queries, static_cast<uint32_t>(nq), k_per_q, ef_per_q);
+        for (std::size_t i = 0; i < tried.size() && i < cap; ++i) {
+            timings[i] = {tried[i].ef_class, tried[i].plan.warps_per_block, tried[i].plan.rows_cap,
+                          tried[i].plan.hash_slots, tried[i].plan.efcap, tried[i].ms};
+        }
+        if (n_out != nullptr) {
+            *n_out = tried.size();
+        }
     });
 }
 

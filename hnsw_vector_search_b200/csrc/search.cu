@@ -226,7 +226,8 @@ __global__ void __launch_bounds__(256) search_kernel(const SearchArgs a) {
     const bool learned = a.stop_enabled != nullptr;
     const bool tracing = a.trace.truth != nullptr;
     const auto* vecs = static_cast<const unsigned char*>(g.vectors);
-    const std::uint32_t nq = a.nq_device != nullptr ? *a.nq_device : a.nq;
+    // A device-side batch size never exceeds the buffers' capacity (a.nq).
+    const std::uint32_t nq = a.nq_device != nullptr ? min(*a.nq_device, a.nq) : a.nq;
     const std::uint32_t hmask = a.hash_slots - 1;
     const int rounds_cap = static_cast<int>(a.rows_cap < 32 ? a.rows_cap : 32);
     const std::uint32_t stride_s = padded_row_stride(g.row_bytes);
@@ -532,8 +533,9 @@ __global__ void __launch_bounds__(256) search_kernel(const SearchArgs a) {
         __syncwarp();
 
         // Optional exact FP32 re-rank of the best candidates (low-precision traversal).
-        if (a.rerank > 0 && P != kFP32) {
-            const int m = min(r, static_cast<int>(a.rerank));
+        const std::uint32_t rerank_n = a.rerank_per_k != 0 ? a.rerank_per_k * k : a.rerank;
+        if (rerank_n > 0 && P != kFP32) {
+            const int m = min(r, static_cast<int>(rerank_n));
             for (int i = lane; i < m; i += 32) {
                 fresh[i] = rid[i] & kIdMask;
             }

@@ -66,7 +66,7 @@ struct SearchArgs {
     const float* queries = nullptr;       // nq rows of qstride floats
     std::uint32_t nq = 0;
     std::uint32_t qstride = 0;
-    const std::uint32_t* nq_device = nullptr;   // batch size read on the device when non-null
+    const std::uint32_t* nq_device = nullptr;   // batch size read on the device (<= nq) when non-null
     const std::uint32_t* k_per_q = nullptr;
     const std::uint32_t* ef_per_q = nullptr;
     std::uint32_t k = 10;
@@ -79,6 +79,8 @@ struct SearchArgs {
     unsigned long long* stats = nullptr;   // kStatCount words or null
     std::uint32_t* claim = nullptr;        // work counter, zeroed before launch
     std::uint32_t rerank = 0;              // re-score this many best in FP32 (0: none)
+    std::uint32_t rerank_per_k = 0;        // non-zero: re-score rerank_per_k * k (rerank >= the
+                                           // largest such width, for the scratch sizing)
     StopNetView stop{};
     const void* stop_enabled = nullptr;    // non-null: learned early termination is on
     float stop_threshold = 0.5F;

@@ -153,6 +153,41 @@ VDX_API vdx_status vdx_search_batch_device_noalloc(const vdx_index* index, const
                                                    uint32_t* d_counts,
                                                    const vdx_search_options* opts, void* stream);
 
+/* --- Uneven batches through a captured CUDA graph (no counterpart in the reference) -------- */
+
+typedef struct vdx_batcher vdx_batcher;
+typedef struct vdx_plan_timing {
+    uint32_t ef_class;          /* the class's largest effective ef */
+    int32_t warps_per_block;
+    uint32_t rows_per_round;
+    uint32_t hash_slots;
+    uint32_t result_capacity;
+    float ms;
+} vdx_plan_timing;
+
+/* A batcher for batches of up to max_queries queries with per-query k <= max_k and
+ * ef <= max_ef: device buffers, pinned staging and the search launches captured once into a
+ * CUDA graph that every batch replays (the kernel reads the batch size, k and ef from device
+ * memory). Queries are split into ef classes (effective ef <= 64, <= 256, <= 1024, ...), each
+ * with its own launch plan, run as concurrent branches of the graph. Results equal
+ * vdx_search_batch of each query with its own k and ef (BF16 / FP8: re-rank width 4 * k).
+ * The batcher keeps the index's device copy as it was: adding to the index afterwards makes
+ * every later run fail with VDX_ERR_INVALID_ARGUMENT. One batch at a time per batcher. */
+VDX_API vdx_status vdx_batcher_create(const vdx_index* index, int32_t device, uint32_t precision,
+                                      uint32_t max_queries, uint32_t max_k, uint32_t max_ef,
+                                      vdx_batcher** out);
+VDX_API void vdx_batcher_free(vdx_batcher* batcher);
+/* One batch, synchronous: queries nq x dim (host), k_per_q, ef_per_q (host, nq each); results
+ * ids / dists nq x max_k, counts nq. */
+VDX_API vdx_status vdx_batcher_run(vdx_batcher* batcher, const float* queries, uint64_t nq,
+                                   const uint32_t* k_per_q, const uint32_t* ef_per_q,
+                                   uint32_t* ids, float* dists, uint32_t* counts);
+/* Times the candidate launch plans on a sample batch, keeps the fastest (and re-captures).
+ * Up to `cap` timings are written to `timings`; *n_out receives how many plans were tried. */
+VDX_API vdx_status vdx_batcher_autotune(vdx_batcher* batcher, const float* queries, uint64_t nq,
+                                        const uint32_t* k_per_q, const uint32_t* ef_per_q,
+                                        vdx_plan_timing* timings, uint64_t cap, uint64_t* n_out);
+
 /* --- Learned early termination (no counterpart in the reference; its training and the
  * in-search network are this library's own) ------------------------------------------------ */
 
