@@ -142,6 +142,23 @@ __device__ __forceinline__ void tmem_ld32(std::uint32_t taddr, std::uint32_t (&r
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+// d0 = fma(c, s0, b0), d1 = fma(c, s1, b1) in one paired instruction (each half rounded as a
+// scalar fma).
+__device__ __forceinline__ void fma2(float& d0, float& d1, float c, float s0, float s1, float b0,
+                                     float b1) {
+    std::uint64_t cc, ss, bb, dd;
+    asm("mov.b64 %0, {%1, %1};" : "=l"(cc) : "f"(c));
+    asm("mov.b64 %0, {%1, %2};" : "=l"(ss) : "f"(s0), "f"(s1));
+    asm("mov.b64 %0, {%1, %2};" : "=l"(bb) : "f"(b0), "f"(b1));
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(dd) : "l"(cc), "l"(ss), "l"(bb));
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(d0), "=f"(d1) : "l"(dd));
+}
+__device__ __forceinline__ float max3(float a, float b, float c) {
+    float d;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+
 // Order-preserving map of floats to u32 (so atomicMax on the key is max on the float).
 __device__ __forceinline__ std::uint32_t float_to_key(float f) {
     const std::uint32_t u = __float_as_uint(f);
@@ -240,9 +257,6 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (warp == 0 && lane == 0) {
         // TMA producer.
         std::uint32_t it = 0, item_idx = 0;
-        std::uint32_t last_full[8];
-        std::uint32_t last_parity[8];
-        std::uint32_t outstanding = 0;
         bool ok = true;
         for (std::uint32_t item = blockIdx.x; ok && item < items; item += gridDim.x, ++item_idx) {
             const std::uint32_t qt = item % p.qtiles;
@@ -282,16 +296,14 @@ __global__ void __launch_bounds__(kThreads, 1)
                                     y, full(s));
                     }
                 }
-                last_full[s] = full(s);
-                last_parity[s] = ph;
-                outstanding = min(outstanding + 1, S);
             }
         }
         if (!ok) {
-            // Let every copy this thread issued land before the CTA exits (bounded).
-            for (std::uint32_t s = 0; s < outstanding; ++s) {
+            // Let every copy this thread issued land before the CTA exits (bounded): the loads
+            // of the last min(S, it) tiles, tile i on stage i % S with phase parity (i / S) & 1.
+            for (std::uint32_t i = it > S ? it - S : 0; i < it; ++i) {
                 const std::uint64_t t0 = now_ns();
-                while (!mbar_try(last_full[s], last_parity[s]) && now_ns() - t0 < kWaitNs) {
+                while (!mbar_try(full(i % S), (i / S) & 1u) && now_ns() - t0 < kWaitNs) {
                 }
             }
         }
@@ -351,12 +363,13 @@ __global__ void __launch_bounds__(kThreads, 1)
     } else if (warp >= 4) {
         // Epilogue: thread e owns query row e of the tile (TMEM lane e). It works in score space,
         // t = 2 q.x - ||x||^2 (L2) or t = q.x (inner product), larger is closer; the per-row
-        // bias (||x||^2, or 0; +inf for padding rows) is read 32 at a time with broadcast 16-byte
-        // loads, and a chunk of 32 scores enters the insertion path only if its best score can
-        // beat the list's current worst.
+        // offset (-||x||^2, or -0; -inf for padding rows) is read 32 at a time with broadcast
+        // 16-byte loads, and a group of 32 scores enters the insertion path only if its best
+        // score can beat the list's current worst.
         const std::uint32_t e = threadIdx.x - 128;
         const std::uint32_t lane_base = static_cast<std::uint32_t>((warp & 3) * 32) << 16;
         const bool l2 = p.metric == 0;
+        const float c2 = l2 ? 2.0F : 1.0F;
         std::uint32_t acc_it = 0;
         for (std::uint32_t item = blockIdx.x; item < items; item += gridDim.x) {
             const std::uint32_t qt = item % p.qtiles;
@@ -389,33 +402,36 @@ __global__ void __launch_bounds__(kThreads, 1)
                         mbar_arrive(tempty0 + 8 * b);
                     }
                     const std::uint32_t id0 = row0 + t * kBN + cc * 32;
-                    const float4* bias4 = reinterpret_cast<const float4*>(p.xnorm + id0);
+                    const float4* nb4 = reinterpret_cast<const float4*>(p.xnorm + id0);
+                    // t = c * s + nb with c = 2 (L2) or 1 and nb = -||x||^2 (L2), -0 (inner
+                    // product) or -inf (padding rows): two scores per f32x2 FMA, each rounded
+                    // like a scalar fmaf. Everything stays in registers (static indices only).
                     float sc[32];
-                    std::uint32_t mask = 0;
 #pragma unroll
                     for (int q4 = 0; q4 < 8; ++q4) {
-                        const float4 bv = __ldg(bias4 + q4);
-                        const float bb[4] = {bv.x, bv.y, bv.z, bv.w};
-#pragma unroll
-                        for (int u = 0; u < 4; ++u) {
-                            const float sv = __uint_as_float(r[4 * q4 + u]);
-                            const float v = l2 ? __fmaf_rn(2.0F, sv, -bb[u]) : __fsub_rn(sv, bb[u]);
-                            sc[4 * q4 + u] = v;
-                            mask |= (v >= thr ? 1u : 0u) << (4 * q4 + u);
-                        }
+                        const float4 bv = __ldg(nb4 + q4);
+                        fma2(sc[4 * q4], sc[4 * q4 + 1], c2, __uint_as_float(r[4 * q4]),
+                             __uint_as_float(r[4 * q4 + 1]), bv.x, bv.y);
+                        fma2(sc[4 * q4 + 2], sc[4 * q4 + 3], c2, __uint_as_float(r[4 * q4 + 2]),
+                             __uint_as_float(r[4 * q4 + 3]), bv.z, bv.w);
                     }
-                    if (!live) {
+                    // Best of the 32 with three-input max; most groups stop here.
+                    float m8[11];
+#pragma unroll
+                    for (int i = 0; i < 10; ++i) {
+                        m8[i] = max3(sc[3 * i], sc[3 * i + 1], sc[3 * i + 2]);
+                    }
+                    m8[10] = fmaxf(sc[30], sc[31]);
+                    const float mx = max3(max3(m8[0], m8[1], m8[2]), max3(m8[3], m8[4], m8[5]),
+                                          max3(max3(m8[6], m8[7], m8[8]), m8[9], m8[10]));
+                    if (!live || !(mx >= thr)) {
                         continue;
                     }
-                    // One iteration per candidate that may qualify; the bound only rises.
-                    while (mask != 0) {
-                        const int j = __ffs(mask) - 1;
-                        mask &= mask - 1;
-                        float v = sc[0];
+                    // Rare path: each score that may qualify, in column order; the bound only
+                    // rises. Static indices keep the scores in registers.
 #pragma unroll
-                        for (int jj = 1; jj < 32; ++jj) {
-                            v = jj == j ? sc[jj] : v;
-                        }
+                    for (int j = 0; j < 32; ++j) {
+                        const float v = sc[j];
                         const std::uint32_t id = id0 + static_cast<std::uint32_t>(j);
                         if (!(v > thr || (v == thr && id < thr_i))) {
                             continue;
@@ -578,12 +594,13 @@ __global__ void prep_rows_kernel(const float* src, std::uint32_t src_stride, std
     }
 }
 
-// The epilogue's per-row score bias: ||x||^2 for L2, 0 for inner product, +inf past the end.
+// The epilogue's per-row score offset, added to c * q.x: -||x||^2 for L2, -0 for inner product
+// (so the score is q.x - 0 exactly), -inf past the end.
 __global__ void bias_kernel(const float* norm, float* bias, std::uint32_t n, std::uint32_t n_pad,
                             std::uint32_t l2) {
     const std::uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n_pad) {
-        bias[i] = i < n ? (l2 ? norm[i] : 0.0F) : INFINITY;
+        bias[i] = i < n ? (l2 ? -norm[i] : -0.0F) : -INFINITY;
     }
 }
 
