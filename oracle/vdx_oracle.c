@@ -230,7 +230,7 @@ vo_index* vo_index_load(const char* path) {
     ix->layer0 = (uint32_t*)malloc((n * b0 ? n * b0 : 1) * 4);
     ix->upper = (uint32_t*)malloc((ix->upper_blocks * b1 ? ix->upper_blocks * b1 : 1) * 4);
     ix->upper_at = (uint64_t*)malloc((n ? n : 1) * 8);
-    ix->vectors = (float*)malloc((n * ix->dim ? n * ix->dim : 1) * 4);
+    ix->vectors = (float*)malloc((n * ix->dim != 0 ? n * ix->dim : 1) * 4);
     int ok = fread(ix->levels, 1, n, f) == n && fread(ix->layer0, 4, n * b0, f) == n * b0 &&
              fread(ix->upper, 4, ix->upper_blocks * b1, f) == ix->upper_blocks * b1 &&
              fread(ix->vectors, 4, n * ix->dim, f) == n * ix->dim;
