@@ -327,7 +327,7 @@ def main():
                 points[name] = (ef, rec)
                 break
         else:
-            points[name] = (EF_SWEEP[-1], rec)
+            points[name] = (efs[-1], rec)
 
     dev = torch.device("cuda", local)
     q_dev = torch.from_numpy(queries).to(dev)
@@ -378,7 +378,9 @@ def main():
                              "qps": nq * world * args.steps / total, "stats": st.tolist()}
     clock_summary = clocks.summary()
 
-    best = max(results, key=lambda n: results[n]["qps"])
+    # The headline counts only modes that reach the recall target on the test queries.
+    eligible = [n for n in results if results[n]["recall"] >= TARGET_RECALL] or list(results)
+    best = max(eligible, key=lambda n: results[n]["qps"])
     r = results[best]
     st = r["stats"]
     algorithmic = st[4] + st[5] + st[6] + nq * 128 * 4  # links + rows + rerank rows + queries
@@ -447,14 +449,15 @@ def main():
 
 
 def learned_mode(v, ix, base, graph, device) -> dict:
-    """Trains (or loads the cached) learned-termination model for this graph: traces of the
-    plain search at ef = 512 for 20,000 training queries (seed 21, the same mixture as the test
-    queries) judged by exact brute force, this library's training kernels, then the threshold
-    and ef cap calibrated on 5,000 more queries (seed 22) for recall@10 >= 0.955 with BF16
-    traversal. The 10,000 test queries are never used for training or calibration."""
+    """Trains (or loads the cached) learned-termination model for this graph. For each candidate
+    ef cap: traces of the plain search at that cap for 20,000 training queries (seed 21, the
+    same mixture as the test queries) judged by exact brute force, this library's training
+    kernels, then the stop threshold calibrated on 5,000 more queries (seed 22) for
+    recall@10 >= 0.955 with BF16 traversal; the cap whose calibrated search reads the fewest
+    bytes wins. The 10,000 test queries are never used for training or calibration."""
     from hnsw_vector_search_b200 import learned
     from hnsw_vector_search_b200.datasets import integer_clusters
-    path = CACHE / (graph.stem + "_stop_model.npz")
+    path = CACHE / (graph.stem + f"_stop_model_v{learned.MODEL_VERSION}.npz")
     info = {}
     if path.exists():
         model = learned.StopModel.load(path)
@@ -467,27 +470,29 @@ def learned_mode(v, ix, base, graph, device) -> dict:
         cal_q = integer_clusters(CAL_QUERIES, 128, 1000, seed=22, centers_seed=111)
         train_truth, _, _ = bf.search_batch(train_q, K, method="tensor_core")
         cal_truth, _, _ = bf.search_batch(cal_q, K, method="tensor_core")
-        tr = learned.traces(ix, train_q, train_truth, k=K, ef=512, device=device)
-        x, y = learned.training_set(tr)
-        model, losses = learned.train(x, y, tr["proj"], epochs=6)
-        learned.attach(ix, model)
         best = None
-        for cap in (48, 64, 96):
-            thr, rec = learned.calibrate(ix, model, cal_q, cal_truth, K, 0.955, cap,
+        tried = []
+        for cap in (40, 48, 64, 96):
+            tr = learned.traces(ix, train_q, train_truth, k=K, ef=cap, device=device)
+            x, y = learned.training_set(tr)
+            model_c, losses = learned.train(x, y, tr["proj"], epochs=6)
+            thr, rec = learned.calibrate(ix, model_c, cal_q, cal_truth, K, 0.955, cap,
                                          precision="bf16", rerank=40, device=device)
             ix.search_batch(cal_q, K, cap, precision="bf16", rerank=40, learned_stop=True,
                             stop_threshold=thr, device=device)
             work = v.HnswIndex.last_stats()["row_bytes"]
+            tried.append({"ef_cap": cap, "threshold": thr, "calibration_recall": round(rec, 4),
+                          "row_bytes": int(work), "samples": int(len(x)),
+                          "positive_share": round(float(y.mean()), 3)})
             if rec >= 0.955 and (best is None or work < best[2]):
-                best = (thr, cap, work, rec)
+                best = (thr, cap, work, rec, model_c)
         if best is None:
-            best = (0.995, 96, 0, rec)
+            best = (tried[-1]["threshold"], 96, 0, tried[-1]["calibration_recall"], model_c)
+        model = best[4]
         model.threshold, model.ef_cap = best[0], best[1]
         model.save(path)
         info.update({"source": "trained", "train_seconds": round(time.time() - t0, 1),
-                     "samples": int(len(x)), "positive_share": round(float(y.mean()), 3),
-                     "loss_first_last": [float(losses[0]), float(losses[-1])],
-                     "calibration_recall": round(best[3], 4)})
+                     "candidates": tried, "calibration_recall": round(best[3], 4)})
     learned.attach(ix, model)
     info.update({"threshold": model.threshold, "ef_cap": model.ef_cap,
                  "train_queries": TRAIN_QUERIES, "calibration_queries": CAL_QUERIES})

@@ -255,6 +255,111 @@ __device__ __forceinline__ float lane_distance(const float* q, const unsigned ch
     return kL2 ? raw : __fsub_rn(1.0F, raw);
 }
 
+// Paired FP32 arithmetic (sm_100 f32x2): each half is rounded exactly like the scalar
+// instruction, so a pair of accumulator chains gives the same bits as two scalar chains.
+__device__ __forceinline__ std::uint64_t pack2(float a, float b) {
+    std::uint64_t r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ void unpack2(std::uint64_t v, float& a, float& b) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+}
+// acc += (q - x)^2 (kL2) or acc += q * x, on two chains at once.
+template <bool kL2>
+__device__ __forceinline__ void accumulate2(std::uint64_t& acc, std::uint64_t q, std::uint64_t x) {
+    if constexpr (kL2) {
+        std::uint64_t d;
+        asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(q), "l"(x));
+        asm("fma.rn.f32x2 %0, %1, %1, %2;" : "=l"(acc) : "l"(d), "l"(acc));
+    } else {
+        asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(acc) : "l"(q), "l"(x));
+    }
+}
+
+// The raw sum between the query and one row, computed by TWO lanes: `half` 0 runs the
+// reference's accumulator lanes 0..15 (elements 32t + 0..15), `half` 1 lanes 16..31 (elements
+// 32t + 16..31), two chains per paired instruction. Half 0 also runs the 8-element blocks
+// (accumulator lanes 0..7). The tree: each half forms acc[l] + acc[l + 8] for its lanes,
+// half 1 hands its eight sums to half 0 (partner = lane + 16: call with the row's halves in
+// lanes L and L + 16, every lane of the warp converged), which adds them as
+// (acc[l] + acc[l+8]) + (acc[l+16] + acc[l+24]), runs the fixed horizontal tree and the tail in
+// the reference's order. The result is valid in half 0's lane only. Same bits as lane_raw.
+template <int P, bool kL2>
+__device__ __forceinline__ float pair_raw(const float* q, const unsigned char* row,
+                                          std::uint32_t dim, std::uint32_t row_bytes, int half) {
+    constexpr int E = Vec<P>::kPerLoad;
+    const float scale = row_scale<P>(row, row_bytes);
+    std::uint64_t acc[8];
+#pragma unroll
+    for (int l = 0; l < 8; ++l) {
+        acc[l] = 0;  // two +0.0f
+    }
+    const std::uint32_t off = 16u * static_cast<std::uint32_t>(half);
+    std::uint32_t i = 0;
+    for (; dim - i >= 32; i += 32) {
+#pragma unroll
+        for (int u = 0; u < 16; u += E) {
+            float x[E];
+            load16<P>(row, i + off + u, scale, x);
+#pragma unroll
+            for (int v = 0; v < E && u + v < 16; v += 4) {
+                const float4 qv = *reinterpret_cast<const float4*>(q + i + off + u + v);
+                accumulate2<kL2>(acc[(u + v) >> 1], pack2(qv.x, qv.y), pack2(x[v], x[v + 1]));
+                accumulate2<kL2>(acc[((u + v) >> 1) + 1], pack2(qv.z, qv.w), pack2(x[v + 2], x[v + 3]));
+            }
+        }
+    }
+    const std::uint32_t blocks8_end = i + ((dim - i) & ~7u);
+    if (half == 0) {
+        for (std::uint32_t j = i; j < blocks8_end; j += 8) {
+#pragma unroll
+            for (int v = 0; v < 8; v += 2) {
+                accumulate2<kL2>(acc[v >> 1], pack2(q[j + v], q[j + v + 1]),
+                                 pack2(row_elem<P>(row, j + v, scale), row_elem<P>(row, j + v + 1, scale)));
+            }
+        }
+    }
+    float a[16];
+#pragma unroll
+    for (int l = 0; l < 8; ++l) {
+        unpack2(acc[l], a[2 * l], a[2 * l + 1]);
+    }
+    float h[8];
+#pragma unroll
+    for (int l = 0; l < 8; ++l) {
+        h[l] = __fadd_rn(a[l], a[l + 8]);
+    }
+#pragma unroll
+    for (int l = 0; l < 8; ++l) {
+        const float other = __shfl_down_sync(kFull, h[l], 16);
+        h[l] = __fadd_rn(h[l], other);
+    }
+    float s = __fadd_rn(__fadd_rn(__fadd_rn(h[0], h[4]), __fadd_rn(h[2], h[6])),
+                        __fadd_rn(__fadd_rn(h[1], h[5]), __fadd_rn(h[3], h[7])));
+    const std::uint32_t tail = dim - blocks8_end;
+    for (std::uint32_t j = 0; j < tail; ++j) {
+        const float x = row_elem<P>(row, blocks8_end + j, scale);
+        const float y = q[blocks8_end + j];
+        const float av = kL2 ? __fsub_rn(y, x) : y;
+        const float bv = kL2 ? av : x;
+        if (tail >= 4 && j < 4) {
+            s = __fadd_rn(s, __fmul_rn(av, bv));
+        } else {
+            s = __fmaf_rn(av, bv, s);
+        }
+    }
+    return s;
+}
+
+template <int P, bool kL2>
+__device__ __forceinline__ float pair_distance(const float* q, const unsigned char* row,
+                                               std::uint32_t dim, std::uint32_t row_bytes,
+                                               int half) {
+    const float raw = pair_raw<P, kL2>(q, row, dim, row_bytes, half);
+    return kL2 ? raw : __fsub_rn(1.0F, raw);
+}
+
 // A shared-memory row stride for `row_bytes` rows read one row per lane with 16-byte loads:
 // an odd number of 16-byte units, so the 8 lanes of each load phase hit distinct banks.
 __host__ __device__ __forceinline__ std::uint32_t padded_row_stride(std::uint32_t row_bytes) {
@@ -325,6 +430,24 @@ __device__ __forceinline__ bool closer(float da, std::uint32_t ia, float db, std
     return da < db || (da == db && ia < ib);
 }
 
+// Order-preserving map of a float (never NaN) to u32: a < b exactly when key(a) < key(b).
+__device__ __forceinline__ std::uint32_t order_key(float f) {
+    const std::uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float order_key_value(std::uint32_t k) {
+    return __uint_as_float((k & 0x80000000u) ? (k & 0x7FFFFFFFu) : ~k);
+}
+// The warp's smallest (d, tie) pair in (distance, tie) order, in every lane: two redux.sync
+// minima (the distance key, then the tie value among the lanes holding that distance).
+__device__ __forceinline__ void warp_argmin(float d, std::uint32_t tie, float& best_d,
+                                            std::uint32_t& best_tie) {
+    const std::uint32_t kd = order_key(d);
+    const std::uint32_t m = __reduce_min_sync(kFull, kd);
+    best_tie = __reduce_min_sync(kFull, kd == m ? tie : 0xFFFFFFFFu);
+    best_d = order_key_value(m);
+}
+
 // Entries of a sorted result list carry this bit once expanded (ids stay below 2^31).
 constexpr std::uint32_t kExpanded = 0x80000000u;
 constexpr std::uint32_t kIdMask = 0x7FFFFFFFu;
@@ -345,7 +468,10 @@ __device__ __forceinline__ int merge_round(float* rd, std::uint32_t* rid, int& r
         int hi = r;
         while (lo < hi) {
             const int mid = (lo + hi) >> 1;
-            if (closer(rd[mid], rid[mid] & kIdMask, my_d, my_id)) {
+            // closer(R[mid], candidate); the id is read only on a distance tie.
+            const float dm = rd[mid];
+            const bool before = dm < my_d || (dm == my_d && (rid[mid] & kIdMask) < my_id);
+            if (before) {
                 lo = mid + 1;
             } else {
                 hi = mid;
@@ -409,11 +535,8 @@ __device__ __forceinline__ int merge_round(float* rd, std::uint32_t* rid, int& r
         rid[newpos] = my_id;
     }
     r = min(ef, r + na);
-    int low = keep ? newpos : 0x7FFFFFFF;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        low = min(low, __shfl_xor_sync(kFull, low, o));
-    }
+    const int low = static_cast<int>(
+        __reduce_min_sync(kFull, keep ? static_cast<std::uint32_t>(newpos) : 0x7FFFFFFFu));
     __syncwarp();
     return low;
 }

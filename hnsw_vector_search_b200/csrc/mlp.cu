@@ -402,7 +402,10 @@ std::unique_ptr<DeviceStopNet> upload_stop_net(const float* weights, const float
     gpu::use_device(device);
     auto net = std::make_unique<DeviceStopNet>();
     net->device = device;
-    // Layout: bf16 w1 [768], w2 [4096], w3 [64] (u16), then FP32 b1, b2, b3, mean, inv_std, proj.
+    // Layout, for a warp whose lane L owns hidden units L and L + 32 of both layers: bf16 pairs
+    // (unit L in the low half, unit L + 32 in the high half) — w1 as [32 lanes][12 features],
+    // w2 as [16 groups of 4 inputs][32 lanes][4 inputs] (one 16-byte load per lane per group),
+    // w3 as [32 lanes] — then FP32 b1, b2, b3, mean, inv_std, proj.
     const std::size_t n16 = H * F + H * H + H;
     const std::size_t off32 = (n16 * 2 + 255) / 256 * 256;
     const std::size_t n32 = H + H + 1 + F + F;
@@ -416,9 +419,20 @@ std::unique_ptr<DeviceStopNet> upload_stop_net(const float* weights, const float
         const std::uint32_t r = u + 0x7FFFu + ((u >> 16) & 1u);
         return static_cast<std::uint16_t>(r >> 16);
     };
-    for (int i = 0; i < H * F; ++i) h16[i] = bf(weights[kOffW1 + i]);
-    for (int i = 0; i < H * H; ++i) h16[H * F + i] = bf(weights[kOffW2 + i]);
-    for (int i = 0; i < H; ++i) h16[H * F + H * H + i] = bf(weights[kOffW3 + i]);
+    const int half = H / 2;
+    for (int l = 0; l < half; ++l) {
+        for (int c = 0; c < F; ++c) {
+            h16[2 * (l * F + c)] = bf(weights[kOffW1 + l * F + c]);
+            h16[2 * (l * F + c) + 1] = bf(weights[kOffW1 + (l + half) * F + c]);
+        }
+        for (int i = 0; i < H; ++i) {
+            const std::size_t at = H * F + 2 * ((static_cast<std::size_t>(i / 4) * half + l) * 4 + i % 4);
+            h16[at] = bf(weights[kOffW2 + l * H + i]);
+            h16[at + 1] = bf(weights[kOffW2 + (l + half) * H + i]);
+        }
+        h16[H * F + H * H + 2 * l] = bf(weights[kOffW3 + l]);
+        h16[H * F + H * H + 2 * l + 1] = bf(weights[kOffW3 + l + half]);
+    }
     auto* h32 = reinterpret_cast<float*>(host.data() + off32);
     std::memcpy(h32, weights + kOffB1, H * 4);
     std::memcpy(h32 + H, weights + kOffB2, H * 4);

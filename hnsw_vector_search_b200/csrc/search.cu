@@ -136,10 +136,13 @@ __device__ __forceinline__ float sgnlog(float x) { return copysignf(log1pf(fabsf
 // The 12 features of a query's search state after `hops` expansions (the model's inputs):
 //   0 log(1 + |q|)                      1 signed log of the layer-0 entry distance
 //   2 log(1 + (d_k - d_1) / |d_1|)      3..5 relative drop of d_k over the last 4 / 8 / 16
-//   6 log(1 + hops)                     7 log(1 + |R| / k)          8..11 query projections
+//   6 log(1 + hops)                     7 log(1 + expansions since d_k last improved)
+//   8..11 query projections
+// None depends on ef, so a model trained on traces at one ef cap reads the same features at
+// another. Called by every lane (the ballot of feature 7 needs the whole warp).
 __device__ __forceinline__ void stop_features(float* f, float qlen, float d_entry, const float* proj,
                                               const float* rd, int r, int k, const float* hist,
-                                              int hops) {
+                                              int hops, int lane) {
     const int kk = r < k ? r : k;
     const float d1 = rd[0];
     const float dk = rd[kk - 1];
@@ -155,19 +158,23 @@ __device__ __forceinline__ void stop_features(float* f, float qlen, float d_entr
         f[3 + w] = fminf(fmaxf(drop, -10.0F), 10.0F);
     }
     f[6] = log1pf(static_cast<float>(hops));
-    f[7] = log1pf(static_cast<float>(r) / static_cast<float>(k));
+    // hist[(hops - 1 - j) % 32] is d_k after expansion hops - j; count the latest expansions
+    // that left it unchanged (at most 31).
+    const int span = hops < kHist ? hops : kHist;
+    const bool same = lane < span && hist[(hops - 1 - lane) & (kHist - 1)] == dk;
+    const std::uint32_t run = __ballot_sync(kFull, same);
+    const int unchanged = (~run == 0u ? 32 : __ffs(~run) - 1) - 1;
+    f[7] = log1pf(static_cast<float>(unchanged > 0 ? unchanged : 0));
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
         f[8 + i] = proj[i];
     }
 }
 
-__device__ __forceinline__ float bf16_bits(std::uint16_t b) {
-    return __uint_as_float(static_cast<std::uint32_t>(b) << 16);
-}
-
 // P(converged) of the network for features f (identical in every lane); h1 is 64 floats of
-// per-warp shared scratch.
+// per-warp shared scratch. Lane L computes hidden units L and L + 32 of both layers from the
+// packed bf16 pairs (see upload_stop_net), the two chains side by side in the same order as a
+// unit-by-unit evaluation.
 __device__ __forceinline__ float stop_probability(const StopNetView& net, const float* f, float* h1,
                                                   int lane) {
     float x[kFeatures];
@@ -175,12 +182,18 @@ __device__ __forceinline__ float stop_probability(const StopNetView& net, const 
     for (int c = 0; c < kFeatures; ++c) {
         x[c] = (f[c] - net.mean[c]) * net.inv_std[c];
     }
+    const uint4* w1 = reinterpret_cast<const uint4*>(net.w1) + lane * (kFeatures / 4);
     float a0 = net.b1[lane];
     float a1 = net.b1[lane + 32];
 #pragma unroll
-    for (int c = 0; c < kFeatures; ++c) {
-        a0 = fmaf(bf16_bits(net.w1[lane * kFeatures + c]), x[c], a0);
-        a1 = fmaf(bf16_bits(net.w1[(lane + 32) * kFeatures + c]), x[c], a1);
+    for (int c4 = 0; c4 < kFeatures / 4; ++c4) {
+        const uint4 w = __ldg(w1 + c4);
+        const std::uint32_t ws[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            a0 = fmaf(__uint_as_float(ws[u] << 16), x[4 * c4 + u], a0);
+            a1 = fmaf(__uint_as_float(ws[u] & 0xFFFF0000u), x[4 * c4 + u], a1);
+        }
     }
     __syncwarp();
     h1[lane] = fmaxf(a0, 0.0F);
@@ -188,15 +201,22 @@ __device__ __forceinline__ float stop_probability(const StopNetView& net, const 
     __syncwarp();
     float z0 = net.b2[lane];
     float z1 = net.b2[lane + 32];
-    const std::uint16_t* r0 = net.w2 + lane * kHidden;
-    const std::uint16_t* r1 = net.w2 + (lane + 32) * kHidden;
-#pragma unroll 8
-    for (int i = 0; i < kHidden; ++i) {
-        const float h = h1[i];
-        z0 = fmaf(bf16_bits(r0[i]), h, z0);
-        z1 = fmaf(bf16_bits(r1[i]), h, z1);
+    const uint4* w2 = reinterpret_cast<const uint4*>(net.w2) + lane;
+#pragma unroll 4
+    for (int g4 = 0; g4 < kHidden / 4; ++g4) {
+        const uint4 w = __ldg(w2 + g4 * 32);
+        const float4 h = *reinterpret_cast<const float4*>(h1 + 4 * g4);
+        const std::uint32_t ws[4] = {w.x, w.y, w.z, w.w};
+        const float hs[4] = {h.x, h.y, h.z, h.w};
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            z0 = fmaf(__uint_as_float(ws[u] << 16), hs[u], z0);
+            z1 = fmaf(__uint_as_float(ws[u] & 0xFFFF0000u), hs[u], z1);
+        }
     }
-    float part = bf16_bits(net.w3[lane]) * fmaxf(z0, 0.0F) + bf16_bits(net.w3[lane + 32]) * fmaxf(z1, 0.0F);
+    const std::uint32_t w3 = reinterpret_cast<const std::uint32_t*>(net.w3)[lane];
+    float part = __uint_as_float(w3 << 16) * fmaxf(z0, 0.0F) +
+                 __uint_as_float(w3 & 0xFFFF0000u) * fmaxf(z1, 0.0F);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         part += __shfl_xor_sync(kFull, part, o);
@@ -229,9 +249,15 @@ __global__ void __launch_bounds__(256) search_kernel(const SearchArgs a) {
     // A device-side batch size never exceeds the buffers' capacity (a.nq).
     const std::uint32_t nq = a.nq_device != nullptr ? min(*a.nq_device, a.nq) : a.nq;
     const std::uint32_t hmask = a.hash_slots - 1;
-    const int rounds_cap = static_cast<int>(a.rows_cap < 32 ? a.rows_cap : 32);
+    // Two lanes score each row (pair_distance), so a round stages at most 16 rows.
+    const int rounds_cap = static_cast<int>(a.rows_cap < 16 ? a.rows_cap : 16);
     const std::uint32_t stride_s = padded_row_stride(g.row_bytes);
     const int shift = chunk_shift(g.row_bytes);
+    // The row this lane's pair scores: a round holds at most rounds_cap rows, so pairs past it
+    // re-read the last row (their results are masked) instead of reading past the buffer.
+    const unsigned char* const my_row =
+        rows + static_cast<std::uint32_t>(min(lane & 15, rounds_cap - 1)) * stride_s;
+    const int half = lane >> 4;
 
     unsigned long long c_exp = 0, c_d0 = 0, c_du = 0, c_lb = 0, c_rb = 0, c_rr = 0, c_dup = 0,
                        c_pf = 0, c_q = 0, c_stop = 0;
@@ -357,21 +383,18 @@ __global__ void __launch_bounds__(256) search_kernel(const SearchArgs a) {
                     gather_rows(rows, stride_s, vecs, fresh + s0, cnt, g.row_bytes, shift, lane);
                     cp_async_wait<0>();
                     __syncwarp();
+                    const float pd = pair_distance<P, kL2>(q, my_row, g.dim, g.row_bytes, half);
                     float d = INFINITY;
                     int idx = 0x7FFFFFFF;
                     if (lane < cnt) {
-                        d = lane_distance<P, kL2>(q, rows + lane * stride_s, g.dim, g.row_bytes);
+                        d = pd;
                         idx = s0 + lane;
                     }
                     // The first strict minimum in link order: smallest (distance, position).
-#pragma unroll
-                    for (int o = 16; o > 0; o >>= 1) {
-                        const float od = __shfl_xor_sync(kFull, d, o);
-                        const int oi = __shfl_xor_sync(kFull, idx, o);
-                        if (od < d || (od == d && oi < idx)) {
-                            d = od;
-                            idx = oi;
-                        }
+                    {
+                        std::uint32_t bidx;
+                        warp_argmin(d, static_cast<std::uint32_t>(idx), d, bidx);
+                        idx = static_cast<int>(bidx);
                     }
                     if (d < best_d) {
                         best_d = d;
@@ -436,19 +459,20 @@ __global__ void __launch_bounds__(256) search_kernel(const SearchArgs a) {
                 ++c_pf;
             }
             __syncwarp();
-            // Prefetch the links of the next unexpanded entry into the other slot.
-            const int p2 = first_unexpanded(rid, p + 1, r, lane);
             prefetched = kNoId;
-            if (p2 < r) {
-                prefetched = rid[p2] & kIdMask;
-                std::uint32_t* other = lbuf + (slot ^ 1) * g.stride0;
-                const std::uint32_t* src_links =
-                    g.links0 + static_cast<std::size_t>(prefetched) * g.stride0;
-                for (std::uint32_t x = lane; x < (g.stride0 >> 2); x += 32) {
-                    cp_async16(other + 4 * x, src_links + 4 * x);
+            // Starts copying the links of `nxt` (the predicted next expansion) into the other
+            // slot; the copy lands while the current candidates are merged.
+            const auto prefetch_links = [&](std::uint32_t nxt) {
+                prefetched = nxt;
+                if (nxt != kNoId) {
+                    std::uint32_t* other = lbuf + (slot ^ 1) * g.stride0;
+                    const std::uint32_t* src_links = g.links0 + static_cast<std::size_t>(nxt) * g.stride0;
+                    for (std::uint32_t x = lane; x < (g.stride0 >> 2); x += 32) {
+                        cp_async16(other + 4 * x, src_links + 4 * x);
+                    }
+                    cp_async_commit();
                 }
-                cp_async_commit();
-            }
+            };
             // Unvisited neighbors, in link order.
             int f = 0;
             int count = 0;
@@ -476,16 +500,40 @@ __global__ void __launch_bounds__(256) search_kernel(const SearchArgs a) {
                 cp_async_wait<0>();
                 __syncwarp();
                 const bool valid = lane < cnt;
-                float my_d = INFINITY;
-                if (valid) {
-                    my_d = lane_distance<P, kL2>(q, rows + lane * stride_s, g.dim, g.row_bytes);
-                }
+                const float pd = pair_distance<P, kL2>(q, my_row, g.dim, g.row_bytes, half);
+                const float my_d = valid ? pd : INFINITY;
                 const std::uint32_t my_id = valid ? fresh[s0 + lane] : kNoId;
                 c_d0 += cnt;
                 c_rb += static_cast<unsigned long long>(cnt) * g.row_bytes;
                 __syncwarp();
+                if (s0 + rounds_cap >= f) {
+                    // Last round: the next expansion is the closer of R's first unexpanded entry
+                    // and this round's best candidate (when the merge will admit it). Exact except
+                    // when that candidate duplicates an expanded entry (a visited-filter miss);
+                    // then the next step fetches its links itself.
+                    float bd;
+                    std::uint32_t bi;
+                    warp_argmin(my_d, my_id, bd, bi);
+                    const bool admissible =
+                        bi != kNoId && (r < ef || closer(bd, bi, rd[r - 1], rid[r - 1] & kIdMask));
+                    const int pu = first_unexpanded(rid, scan, r, lane);
+                    std::uint32_t nxt = admissible ? bi : kNoId;
+                    if (pu < r) {
+                        const std::uint32_t ui = rid[pu] & kIdMask;
+                        if (!admissible || closer(rd[pu], ui, bd, bi)) {
+                            nxt = ui;
+                        }
+                    }
+                    __syncwarp();
+                    prefetch_links(nxt);
+                }
                 const int low = merge_round(rd, rid, r, ef, my_d, my_id, valid, ap, lane, c_dup);
                 scan = min(scan, low);
+            }
+            if (f == 0) {
+                // Nothing scored: the next expansion is R's first unexpanded entry.
+                const int pu = first_unexpanded(rid, scan, r, lane);
+                prefetch_links(pu < r ? rid[pu] & kIdMask : kNoId);
             }
             slot ^= 1;
             ++hops;
@@ -497,7 +545,7 @@ __global__ void __launch_bounds__(256) search_kernel(const SearchArgs a) {
                 __syncwarp();
                 if ((hops & 7) == 0) {
                     float f[kFeatures];
-                    stop_features(f, qlen, d_entry, proj, rd, r, static_cast<int>(k), hist, hops);
+                    stop_features(f, qlen, d_entry, proj, rd, r, static_cast<int>(k), hist, hops, lane);
                     if (tracing && trace_points < a.trace.max_points) {
                         const std::size_t at = static_cast<std::size_t>(qi) * a.trace.max_points + trace_points;
                         if (lane < kFeatures) {

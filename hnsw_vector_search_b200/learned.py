@@ -5,11 +5,11 @@ reads a query's search state every 8 expansions and stops the layer-0 beam once 
 top k has converged; ef stays the hard cap, so the plain ef-bounded search is the fallback.
 
 Pipeline (all heavy work on the GPU, through the C ABI):
-  1. traces   plain search of training queries at a large ef (512); every 8 expansions the
-              12 features and how many of the current top k are true neighbors (exact brute
-              force is the judge), and the final count;
+  1. traces   plain search of training queries at the ef cap the model will run under; every 8
+              expansions the 12 features and how many of the current top k are true neighbors
+              (exact brute force is the judge), and the final count;
   2. labels   a checkpoint is "converged" when its hit count already equals the final one:
-              stopping there would lose nothing against searching on to ef = 512;
+              stopping there would lose nothing against searching on to the cap;
   3. train    vdx_mlp_train: this library's forward / backward / Adam kernels;
   4. calibrate  the stop threshold is the smallest one whose recall on held-out queries meets
               the target at the chosen ef cap.
@@ -29,7 +29,7 @@ from . import _P, _U32, _U64, _raise, _ptr, lib
 
 FEATURES = 12
 PARAMS = 5057
-MODEL_VERSION = 1
+MODEL_VERSION = 2
 
 
 def _bind():
@@ -166,8 +166,9 @@ def calibrate(index, model: StopModel, queries: np.ndarray, truth: np.ndarray, k
     """The smallest threshold (fastest stopping) whose recall@k on `queries` meets `target` at
     ef cap `ef_cap`; returns (threshold, recall). Falls back to the largest candidate."""
     attach(index, model)
-    cands = thresholds if thresholds is not None else [0.5, 0.6, 0.7, 0.8, 0.85, 0.9, 0.93, 0.95,
-                                                       0.97, 0.98, 0.99, 0.995]
+    cands = thresholds if thresholds is not None else [0.05, 0.1, 0.2, 0.3, 0.4, 0.5, 0.6, 0.7,
+                                                       0.8, 0.85, 0.9, 0.93, 0.95, 0.97, 0.98,
+                                                       0.99, 0.995]
     best = None
     for t in sorted(cands):
         ids, _, _ = index.search_batch(queries, k, ef_cap, learned_stop=True, stop_threshold=t,
