@@ -580,7 +580,10 @@ def study_uneven(args, v, torch):
     it, all through host buffers (copies in the timed region), closed loop:
       per_request  HnswIndex.search_batch per request (the plain batch API);
       batcher      one captured-graph replay per request (ef classes, autotuned plans);
-      packed       consecutive requests packed into batches of <= 4096 queries, one replay each.
+      packed       consecutive requests packed into batches of <= 4096 queries, one replay each;
+      pipelined    the packed batches spread over 4 batchers (4 streams), up to 4 in flight: the
+                   host stages batch b + 1 while the GPU runs batch b, and one batch's tail
+                   overlaps the next one's start.
     Reported: queries/s over the stream and per-request latency (p50 / p99, from the start of the
     call that serves the request to its results on the host). Every request's rows are checked
     against the plain search on a sample."""
@@ -604,7 +607,8 @@ def study_uneven(args, v, torch):
     total_q = int(offs[-1])
     log(f"uneven stream: {len(requests)} requests, {total_q} queries")
 
-    bt = v.Batcher(ix, max_queries=4096, max_k=100, max_ef=4 * 100 + 256)
+    bts = [v.Batcher(ix, max_queries=4096, max_k=100, max_ef=4 * 100 + 256) for _ in range(4)]
+    bt = bts[0]
 
     def pack(reqs):
         batches, cur, cur_n = [], [], 0
@@ -626,6 +630,8 @@ def study_uneven(args, v, torch):
     t0 = time.time()
     tuned = bt.autotune(sq, sk, se)
     tune_s = time.time() - t0
+    for other in bts[1:]:
+        other.autotune(sq, sk, se)
     chosen = {}
     for t in tuned:
         c = chosen.get(t["ef_class"])
@@ -645,14 +651,30 @@ def study_uneven(args, v, torch):
         lat = np.zeros(len(requests))
         torch.cuda.synchronize()
         t_all = time.perf_counter()
+        def packed(b):
+            q = np.concatenate([requests[i][0] for i in b])
+            kk = np.concatenate([np.full(len(requests[i][0]), requests[i][1], np.uint32) for i in b])
+            ee = np.concatenate([np.full(len(requests[i][0]), requests[i][2], np.uint32) for i in b])
+            return q, kk, ee
         if mode == "packed":
             for b in batches:
                 t0 = time.perf_counter()
-                q = np.concatenate([requests[i][0] for i in b])
-                kk = np.concatenate([np.full(len(requests[i][0]), requests[i][1], np.uint32) for i in b])
-                ee = np.concatenate([np.full(len(requests[i][0]), requests[i][2], np.uint32) for i in b])
-                bt.run(q, kk, ee)
+                bt.run(*packed(b))
                 lat[b] = time.perf_counter() - t0
+        elif mode == "pipelined":
+            pending = [None] * len(bts)
+            for n_b, b in enumerate(batches):
+                slot = n_b % len(bts)
+                if pending[slot] is not None:
+                    bts[slot].wait()
+                    lat[pending[slot][0]] = time.perf_counter() - pending[slot][1]
+                t0 = time.perf_counter()
+                bts[slot].submit(*packed(b))
+                pending[slot] = (b, t0)
+            for slot, pend in enumerate(pending):
+                if pend is not None:
+                    bts[slot].wait()
+                    lat[pend[0]] = time.perf_counter() - pend[1]
         else:
             for i, (q, k, ef) in enumerate(requests):
                 t0 = time.perf_counter()
@@ -668,7 +690,7 @@ def study_uneven(args, v, torch):
 
     out = {}
     with Clocks(0) as clocks:
-        for mode in ("per_request", "batcher", "packed"):
+        for mode in ("per_request", "batcher", "packed", "pipelined"):
             serve(mode)  # warm-up pass
             out[mode] = serve(mode)
     line = {"study": "uneven", "workload": f"{n} x 96 IP, 4,096 clusters (log-normal scales), "
@@ -719,7 +741,7 @@ def study_precision(args, v, torch):
 
     modes = [("fp32", {}), ("bf16+rerank40", {"precision": "bf16", "rerank": 40}),
              ("fp8+rerank40", {"precision": "fp8", "rerank": 40}),
-             ("bf16", {"precision": "bf16", "rerank": 0}), ("fp8", {"precision": "fp8", "rerank": 0})]
+             ("bf16", {"precision": "bf16", "rerank": "none"}), ("fp8", {"precision": "fp8", "rerank": "none"})]
     table = {}
     for name, o in modes:
         for ef in (16, 32, 64, 128, 256, 512):

@@ -97,6 +97,8 @@ def lib() -> ctypes.CDLL:
         "vdx_batcher_free": (None, [_P]),
         "vdx_batcher_run": (ctypes.c_int, [_P, _P, _U64, _P, _P, _P, _P, _P]),
         "vdx_batcher_autotune": (ctypes.c_int, [_P, _P, _U64, _P, _P, _P, _U64, ctypes.POINTER(_U64)]),
+        "vdx_batcher_submit": (ctypes.c_int, [_P, _P, _U64, _P, _P]),
+        "vdx_batcher_wait": (ctypes.c_int, [_P, _P, _P, _P]),
         "vdx_host_l2": (_F, [_P, _P, _U64]),
         "vdx_host_ip": (_F, [_P, _P, _U64]),
         "vdx_xxh64": (_U64, [_P, _U64, _U64]),
@@ -134,8 +136,10 @@ def _rows(data, dim: int) -> np.ndarray:
 
 
 def _options(precision="fp32", rerank=0, learned_stop=False, stop_threshold=0.5, device=0):
+    """rerank: 0 = 4k candidates re-scored in FP32 (BF16 / FP8), "none" = no re-rank."""
+    rr = 0xFFFFFFFF if rerank == "none" else int(rerank)
     return SearchOptions(PRECISIONS[precision] if isinstance(precision, str) else int(precision),
-                         int(rerank), 1 if learned_stop else 0, float(stop_threshold), int(device))
+                         rr, 1 if learned_stop else 0, float(stop_threshold), int(device))
 
 
 class HnswIndex:
@@ -293,6 +297,26 @@ class Batcher:
         c = np.empty(nq, np.uint32)
         _raise(lib().vdx_batcher_run(self._h, _ptr(q), nq, _ptr(kk), _ptr(ee), _ptr(ids), _ptr(d),
                                      _ptr(c)))
+        return ids, d, c
+
+    def submit(self, queries, k, ef) -> None:
+        """Starts a batch without waiting; `wait` returns its results. One batch in flight per
+        batcher (several batchers keep several in flight)."""
+        q = _rows(queries, self.index.dim)
+        nq = q.shape[0]
+        kk, ee = self._per_query(k, nq), self._per_query(ef, nq)
+        _raise(lib().vdx_batcher_submit(self._h, _ptr(q), nq, _ptr(kk), _ptr(ee)))
+        self._pending = nq
+
+    def wait(self):
+        nq = getattr(self, "_pending", None)
+        if nq is None:
+            raise ValueError("Batcher.wait: no batch was submitted")
+        self._pending = None
+        ids = np.empty((nq, self.max_k), np.uint32)
+        d = np.empty((nq, self.max_k), np.float32)
+        c = np.empty(nq, np.uint32)
+        _raise(lib().vdx_batcher_wait(self._h, _ptr(ids), _ptr(d), _ptr(c)))
         return ids, d, c
 
     def autotune(self, queries, k, ef) -> list[dict]:

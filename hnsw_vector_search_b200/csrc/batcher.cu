@@ -259,10 +259,12 @@ void Batcher::stage(const float* queries, std::uint32_t nq, const std::uint32_t*
     }
 }
 
-void Batcher::run(const float* queries, std::uint32_t nq, const std::uint32_t* k,
-                  const std::uint32_t* ef, std::uint32_t* ids, float* dists,
-                  std::uint32_t* counts) {
+void Batcher::submit(const float* queries, std::uint32_t nq, const std::uint32_t* k,
+                     const std::uint32_t* ef) {
     gpu::use_device(device);
+    if (in_flight) {
+        throw std::invalid_argument("Batcher::submit: the previous batch has not been collected (wait)");
+    }
     stage(queries, nq, k, ef);
     gpu::check(cudaGraphLaunch(exec, stream), "graph launch");
     for (EfClass& c : classes) {
@@ -278,6 +280,15 @@ void Batcher::run(const float* queries, std::uint32_t nq, const std::uint32_t* k
         gpu::check(cudaMemcpyAsync(c.h_work, c.d_work, kWorkWords * 4, cudaMemcpyDeviceToHost, stream),
                    "copy status");
     }
+    in_flight = true;
+}
+
+void Batcher::wait(std::uint32_t* ids, float* dists, std::uint32_t* counts) {
+    gpu::use_device(device);
+    if (!in_flight) {
+        throw std::invalid_argument("Batcher::wait: no batch was submitted");
+    }
+    in_flight = false;
     gpu::check(cudaStreamSynchronize(stream), "batch");
     for (const EfClass& c : classes) {
         gpu::raise_status(c.h_work[0], "Batcher::run");
@@ -290,6 +301,13 @@ void Batcher::run(const float* queries, std::uint32_t nq, const std::uint32_t* k
             counts[i] = c.h_counts[j];
         }
     }
+}
+
+void Batcher::run(const float* queries, std::uint32_t nq, const std::uint32_t* k,
+                  const std::uint32_t* ef, std::uint32_t* ids, float* dists,
+                  std::uint32_t* counts) {
+    submit(queries, nq, k, ef);
+    wait(ids, dists, counts);
 }
 
 float Batcher::time_plan(const EfClass& c, const SearchPlan& p, int reps) {
@@ -315,6 +333,9 @@ float Batcher::time_plan(const EfClass& c, const SearchPlan& p, int reps) {
 std::vector<TunedPlan> Batcher::autotune(const float* queries, std::uint32_t nq,
                                          const std::uint32_t* k, const std::uint32_t* ef) {
     gpu::use_device(device);
+    if (in_flight) {
+        throw std::invalid_argument("Batcher::autotune: a batch is in flight (wait first)");
+    }
     stage(queries, nq, k, ef);
     gpu::check(cudaStreamSynchronize(stream), "stage");
     std::vector<TunedPlan> tried;

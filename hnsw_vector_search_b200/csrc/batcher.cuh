@@ -46,6 +46,13 @@ struct Batcher {
     // One batch (host buffers): queries nq x dim, per-query k and ef; results nq x max_k.
     void run(const float* queries, std::uint32_t nq, const std::uint32_t* k, const std::uint32_t* ef,
              std::uint32_t* ids, float* dists, std::uint32_t* counts);
+    // The same in two halves: submit stages the batch and enqueues the copies and the graph on
+    // this batcher's stream without waiting (the caller's buffers may be reused at once); wait
+    // blocks until that batch is done and writes its results. One batch in flight per batcher;
+    // several batchers keep several batches in flight.
+    void submit(const float* queries, std::uint32_t nq, const std::uint32_t* k, const std::uint32_t* ef);
+    void wait(std::uint32_t* ids, float* dists, std::uint32_t* counts);
+    bool in_flight = false;
     // Times the candidate plans of every class on this batch, keeps each class's fastest and
     // re-captures the graph.
     std::vector<TunedPlan> autotune(const float* queries, std::uint32_t nq, const std::uint32_t* k,

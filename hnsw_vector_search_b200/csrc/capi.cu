@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cstring>
 #include <exception>
+#include <format>
 #include <new>
 #include <stdexcept>
 #include <string>
@@ -274,7 +275,7 @@ vdx_status vdx_search_batch_device(const vdx_index* index, const float* d_querie
         a.claim = d_work + 2;
         a.stats = reinterpret_cast<unsigned long long*>(d_work + 16);
         const uint32_t kk = std::max<uint32_t>(k_uniform, 1);
-        a.rerank = o.precision == vdx::Precision::FP32 ? 0U : (o.rerank > 0 ? o.rerank : 4 * kk);
+        a.rerank = vdx::rerank_width(o, kk);
         if (o.learned_stop) {
             const vdx::dev::DeviceStopNet& net = h.stop_net(o.device);
             a.stop = net.view;
@@ -291,6 +292,15 @@ vdx_status vdx_search_batch_device(const vdx_index* index, const float* d_querie
 struct vdx_batcher {
     vdx::dev::Batcher b;
 };
+
+namespace {
+void check_batch_size(const vdx_batcher& b, uint64_t nq) {
+    if (nq > b.b.max_queries) {
+        throw std::invalid_argument(
+            std::format("vdx_batcher: batch of {} exceeds the maximum {}", nq, b.b.max_queries));
+    }
+}
+}  // namespace
 
 vdx_status vdx_batcher_create(const vdx_index* index, int32_t device, uint32_t precision,
                               uint32_t max_queries, uint32_t max_k, uint32_t max_ef,
@@ -317,7 +327,24 @@ vdx_status vdx_batcher_run(vdx_batcher* batcher, const float* queries, uint64_t 
         if (nq == 0) {
             return;
         }
+        check_batch_size(*batcher, nq);
         batcher->b.run(queries, static_cast<uint32_t>(nq), k_per_q, ef_per_q, ids, dists, counts);
+    });
+}
+
+vdx_status vdx_batcher_submit(vdx_batcher* batcher, const float* queries, uint64_t nq,
+                              const uint32_t* k_per_q, const uint32_t* ef_per_q) {
+    return guarded([&] {
+        require(batcher, "batcher");
+        check_batch_size(*batcher, nq);
+        batcher->b.submit(queries, static_cast<uint32_t>(nq), k_per_q, ef_per_q);
+    });
+}
+
+vdx_status vdx_batcher_wait(vdx_batcher* batcher, uint32_t* ids, float* dists, uint32_t* counts) {
+    return guarded([&] {
+        require(batcher, "batcher");
+        batcher->b.wait(ids, dists, counts);
     });
 }
 
@@ -326,6 +353,7 @@ vdx_status vdx_batcher_autotune(vdx_batcher* batcher, const float* queries, uint
                                 vdx_plan_timing* timings, uint64_t cap, uint64_t* n_out) {
     return guarded([&] {
         require(batcher, "batcher");
+        check_batch_size(*batcher, nq);
         const auto tried = batcher->b.autotune(queries, static_cast<uint32_t>(nq), k_per_q, ef_per_q);
         for (std::size_t i = 0; i < tried.size() && i < cap; ++i) {
             timings[i] = {tried[i].ef_class, tried[i].plan.warps_per_block, tried[i].plan.rows_cap,

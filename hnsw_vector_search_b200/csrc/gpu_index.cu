@@ -480,9 +480,7 @@ void HnswIndex::search_batch_into(MatrixView<float> queries, std::size_t k, std:
     a.status = ws.small;
     a.claim = ws.small + 2;
     a.stats = reinterpret_cast<unsigned long long*>(ws.small + 16);
-    a.rerank = options.precision == Precision::FP32 ? 0U
-                                                    : (options.rerank > 0 ? options.rerank
-                                                                          : static_cast<std::uint32_t>(4 * k));
+    a.rerank = rerank_width(options, k);
     if (options.learned_stop) {
         const dev::DeviceStopNet& net = stop_net_for(*this, *device_mutex_, stop_net_, options.device, where);
         a.stop = net.view;

@@ -122,7 +122,7 @@ extern "C" vdx_status vdx_search_batch_device_noalloc(
         a.claim = work + 2;
         a.stats = reinterpret_cast<unsigned long long*>(work + 16);
         const std::uint32_t kk = k_uniform > 0 ? k_uniform : 1;
-        a.rerank = o.precision == vdx::Precision::FP32 ? 0U : (o.rerank > 0 ? o.rerank : 4 * kk);
+        a.rerank = vdx::rerank_width(o, kk);
         const std::uint64_t ef_cap = ef_uniform > kk ? ef_uniform : kk;
         const std::uint64_t cap = ef_cap < h.size() ? ef_cap : h.size();
         const vdx::dev::SearchPlan plan = vdx::dev::default_plan(g->view, static_cast<std::uint32_t>(cap));

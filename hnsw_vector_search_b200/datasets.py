@@ -100,6 +100,19 @@ def scaled_clusters(rows: int, dim: int, n_clusters: int, seed: int, centers_see
     return out
 
 
+def mixed_difficulty(queries: np.ndarray, share: float, noise: float, seed: int) -> np.ndarray:
+    """A copy of integer-valued `queries` where a `share` of the rows (chosen with `seed`) get
+    Gaussian noise of standard deviation `noise`, clipped to [0, 255] and rounded: queries that
+    fall between the clusters need a much longer search than the others, the workload learned
+    early termination is for."""
+    g = _rng(seed)
+    out = queries.copy()
+    hard = g.random(len(out)) < share
+    out[hard] = np.rint(np.clip(out[hard] + g.normal(0.0, noise, size=(int(hard.sum()), out.shape[1])),
+                                0.0, 255.0))
+    return out.astype(np.float32)
+
+
 # The workloads, by name: (base, queries) factories.
 def config_small_l2(n_queries: int = 1000):
     """10,000 x 128 L2, 100 isotropic clusters (sigma 12), 1,000 queries."""

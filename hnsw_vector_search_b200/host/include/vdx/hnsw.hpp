@@ -67,7 +67,7 @@ enum class Precision : std::uint8_t {
 struct SearchOptions {
     Precision precision = Precision::FP32;
     // For BF16 / FP8: how many of the best candidates are re-scored in FP32 before the top k is
-    // taken; 0 means 4k.
+    // taken; 0 means 4k, kNoRerank none (the traversal-precision distances are returned).
     std::uint32_t rerank = 0;
     // Learned early termination: a small network, evaluated in the kernel every 8 expansions,
     // stops a query's layer-0 search once it predicts the top k has converged. Needs a model
@@ -76,6 +76,16 @@ struct SearchOptions {
     float stop_threshold = 0.5F;
     int device = 0;
 };
+
+inline constexpr std::uint32_t kNoRerank = 0xFFFFFFFFu;
+
+// The FP32 re-rank width a search with `options` and k uses (0: none).
+inline std::uint32_t rerank_width(const SearchOptions& options, std::size_t k) {
+    if (options.precision == Precision::FP32 || options.rerank == kNoRerank) {
+        return 0;
+    }
+    return options.rerank > 0 ? options.rerank : static_cast<std::uint32_t>(4 * k);
+}
 
 class HnswIndex {
 public:

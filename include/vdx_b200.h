@@ -55,7 +55,7 @@ typedef struct vdx_graph_report {
 
 typedef struct vdx_search_options {
     uint32_t precision;      /* VDX_FP32 (reference-identical results), VDX_BF16, VDX_FP8 */
-    uint32_t rerank;         /* BF16 / FP8: candidates re-scored in FP32; 0 = 4k */
+    uint32_t rerank;         /* BF16 / FP8: candidates re-scored in FP32; 0 = 4k, 0xFFFFFFFF = none */
     uint32_t learned_stop;   /* nonzero: learned early termination (needs a model) */
     float stop_threshold;    /* stop when the network's "converged" probability reaches this */
     int32_t device;
@@ -182,6 +182,15 @@ VDX_API void vdx_batcher_free(vdx_batcher* batcher);
 VDX_API vdx_status vdx_batcher_run(vdx_batcher* batcher, const float* queries, uint64_t nq,
                                    const uint32_t* k_per_q, const uint32_t* ef_per_q,
                                    uint32_t* ids, float* dists, uint32_t* counts);
+/* vdx_batcher_run in two halves, so that several batchers keep several batches in flight:
+ * submit copies the batch into the batcher's pinned staging and enqueues the copies and the graph
+ * on its stream, without waiting (the caller's buffers may be reused at once); wait blocks until
+ * that batch is done and writes ids / dists (nq x max_k) and counts. One batch in flight per
+ * batcher: submit again before wait fails with VDX_ERR_INVALID_ARGUMENT. */
+VDX_API vdx_status vdx_batcher_submit(vdx_batcher* batcher, const float* queries, uint64_t nq,
+                                      const uint32_t* k_per_q, const uint32_t* ef_per_q);
+VDX_API vdx_status vdx_batcher_wait(vdx_batcher* batcher, uint32_t* ids, float* dists,
+                                    uint32_t* counts);
 /* Times the candidate launch plans on a sample batch, keeps the fastest (and re-captures).
  * Up to `cap` timings are written to `timings`; *n_out receives how many plans were tried. */
 VDX_API vdx_status vdx_batcher_autotune(vdx_batcher* batcher, const float* queries, uint64_t nq,

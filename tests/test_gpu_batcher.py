@@ -102,3 +102,23 @@ def test_batcher_rejects_what_does_not_fit(gpu, graph):
         bt.run(bad, 5, 16)
     ids, _, c = bt.run(q[:2], 5, 16)  # still usable after an error
     assert list(c) == [5, 5]
+
+
+@pytest.mark.gpu
+def test_batches_in_flight_on_several_batchers(gpu, graph):
+    """submit / wait on two batchers with both batches in flight give the same rows as run."""
+    a = gpu.Batcher(graph, max_queries=100, max_k=10, max_ef=200)
+    b = gpu.Batcher(graph, max_queries=100, max_k=10, max_ef=200)
+    g = np.random.default_rng(12)
+    qa, qb = integer_matrix(100, 24, seed=41), integer_matrix(60, 24, seed=42)
+    ka, kb = g.integers(1, 11, 100).astype(np.uint32), g.integers(1, 11, 60).astype(np.uint32)
+    ea, eb = g.integers(1, 201, 100).astype(np.uint32), g.integers(1, 201, 60).astype(np.uint32)
+    a.submit(qa, ka, ea)
+    b.submit(qb, kb, eb)
+    with pytest.raises(ValueError):
+        a.submit(qa, ka, ea)  # one batch in flight per batcher
+    got_b, got_a = b.wait(), a.wait()
+    for got, (q, k, e) in ((got_a, (qa, ka, ea)), (got_b, (qb, kb, eb))):
+        want = a.run(q, k, e)
+        for x, y in zip(got, want):
+            np.testing.assert_array_equal(x, y)

@@ -208,6 +208,21 @@ def test_fp8_traversal_with_rerank_keeps_recall(gpu, orc, small_l2):
             assert np.float32(o.l2(queries[q], base[ids8[q, i]])) == d8[q, i]
 
 
+def test_low_precision_without_rerank_returns_traversal_distances(gpu, orc, small_l2):
+    """rerank="none": the returned distances are the traversal-precision ones (FP8 rows, FP32
+    accumulation), within the E4M3 quantization error of the exact distances, and sorted."""
+    path, base, queries = small_l2
+    ix = gpu.HnswIndex.load(path)
+    ids, d, c = ix.search_batch(queries, 10, 64, precision="fp8", rerank="none")
+    ids_rr, d_rr, _ = ix.search_batch(queries, 10, 64, precision="fp8")
+    assert np.all(np.diff(d, axis=1) >= 0)
+    exact = np.array([[np.sum((queries[q].astype(np.float64) - base[i]) ** 2) for i in ids[q]]
+                      for q in range(len(queries))])
+    # E4M3 keeps 3 mantissa bits: each stored component is off by at most 1/16 of itself.
+    assert np.all(np.abs(d - exact) <= 0.25 * exact + 1.0)
+    assert not np.array_equal(d, d_rr)  # the default re-rank really re-scores in FP32
+
+
 def test_device_api_with_per_query_k_and_ef(gpu, small_l2):
     torch = pytest.importorskip("torch")
     path, base, queries = small_l2

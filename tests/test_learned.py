@@ -108,35 +108,56 @@ def test_traces_are_consistent_with_the_plain_search(gpu, small_graph):
     assert np.isfinite(tr["features"][tr["points"] > 0][:, :4]).all()
 
 
+@pytest.fixture(scope="module")
+def mixed_workload(gpu):
+    """200,000 x 128 SIFT-like base (1,000 anisotropic clusters); queries from the same mixture,
+    half of them pushed between the clusters (noise sigma 45), so query difficulty varies."""
+    from hnsw_vector_search_b200.datasets import integer_clusters, mixed_difficulty
+    base = integer_clusters(200_000, 128, 1000, seed=1, centers_seed=111)
+    ix = gpu.HnswIndex(128, "l2", M=16, ef_construction=200)
+    ix.add(base, num_threads=0)
+    bf = gpu.BruteForceIndex(128)
+    bf.add(base)
+
+    def queries(n, seed):
+        q = integer_clusters(n, 128, 1000, seed=seed, centers_seed=111)
+        return mixed_difficulty(q, 0.5, 45.0, seed=seed + 1000)
+    return ix, bf, queries
+
+
 @pytest.mark.gpu
-def test_learned_stop_gains_over_plain_search_at_equal_recall(gpu, small_graph):
-    """Trained on ef = 512 traces of 20,000 queries, calibrated on 2,000 others, evaluated on a
-    third set: at the recall the plain search reaches at ef = 64, the learned stop (ef cap 128)
-    needs fewer layer-0 distance evaluations."""
+def test_learned_stop_gains_over_plain_search_at_equal_recall(gpu, mixed_workload):
+    """Trained on traces at its ef cap (192) for 20,000 queries, its threshold calibrated on
+    3,000 others for recall@10 0.96, evaluated on a third set of 5,000: the learned stop reaches
+    the recall with fewer layer-0 distance evaluations than the plain search needs for the same
+    recall (interpolated along the plain search's ef sweep)."""
     from hnsw_vector_search_b200 import learned
-    from hnsw_vector_search_b200.datasets import integer_clusters
-    ix, base = small_graph
-    mk = lambda n, s: integer_clusters(n, 128, 100, seed=s, centers_seed=101, sigma=12.0)
-    train_q, cal_q, test_q = mk(20_000, 21), mk(2_000, 22), mk(3_000, 23)
-    tr = learned.traces(ix, train_q, truth_of(gpu, base, train_q), k=10, ef=512)
+    ix, bf, queries = mixed_workload
+    train_q, cal_q, test_q = queries(20_000, 21), queries(3_000, 22), queries(5_000, 23)
+    truth = lambda q: bf.search_batch(q, 10, method="tensor_core")[0]  # noqa: E731
+    cap, target = 192, 0.96
+    tr = learned.traces(ix, train_q, truth(train_q), k=10, ef=cap)
     x, y = learned.training_set(tr)
     model, losses = learned.train(x, y, tr["proj"], epochs=6)
     assert losses[-1] < losses[0]
 
-    truth_test = truth_of(gpu, base, test_q)
-    plain = {}
-    for ef in (10, 12, 16, 20, 24, 32, 40, 48, 64):
+    test_truth = truth(test_q)
+    plain = []
+    for ef in (24, 32, 40, 48, 64, 96, 128, 192, 256):
         ids, _, _ = ix.search_batch(test_q, 10, ef)
-        plain[ef] = (learned.recall(ids, truth_test, 10), gpu.HnswIndex.last_stats()["dist_layer0"])
-    target = plain[64][0] - 0.002
-    thr, _ = learned.calibrate(ix, model, cal_q, truth_of(gpu, base, cal_q), 10, target + 0.001, 128)
-    ids, _, _ = ix.search_batch(test_q, 10, 128, learned_stop=True, stop_threshold=thr)
-    rec = learned.recall(ids, truth_test, 10)
+        plain.append((learned.recall(ids, test_truth, 10), gpu.HnswIndex.last_stats()["dist_layer0"]))
+    thr, _ = learned.calibrate(ix, model, cal_q, truth(cal_q), 10, target, cap)
+    ids, _, _ = ix.search_batch(test_q, 10, cap, learned_stop=True, stop_threshold=thr)
+    rec = learned.recall(ids, test_truth, 10)
     work = gpu.HnswIndex.last_stats()["dist_layer0"]
-    plain_work = min(w for r, w in plain.values() if r >= rec - 1e-9) if any(
-        r >= rec - 1e-9 for r, _ in plain.values()) else plain[64][1]
-    report = {"recall_learned": rec, "work_learned": work, "plain": plain, "threshold": thr,
-              "plain_work_at_equal_recall": plain_work, "gain": plain_work / work}
+    plain.sort()
+    plain_work = None
+    for (r0, w0), (r1, w1) in zip(plain, plain[1:]):
+        if r0 <= rec <= r1:
+            plain_work = w0 + (w1 - w0) * (rec - r0) / max(r1 - r0, 1e-12)
+    report = {"recall_learned": rec, "work_learned": work, "threshold": thr, "plain": plain,
+              "plain_work_at_equal_recall": plain_work,
+              "gain": None if plain_work is None else plain_work / work}
     print(json.dumps(report))
-    assert rec >= target - 0.005
-    assert work < plain_work, report
+    assert rec >= target - 0.01, report
+    assert plain_work is not None and plain_work / work >= 1.08, report
