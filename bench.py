@@ -581,9 +581,9 @@ def study_uneven(args, v, torch):
       per_request  HnswIndex.search_batch per request (the plain batch API);
       batcher      one captured-graph replay per request (ef classes, autotuned plans);
       packed       consecutive requests packed into batches of <= 4096 queries, one replay each;
-      pipelined    the packed batches spread over 4 batchers (4 streams), up to 4 in flight: the
-                   host stages batch b + 1 while the GPU runs batch b, and one batch's tail
-                   overlaps the next one's start.
+      pipelined    the packed batches (<= 4096 or <= 1024 queries) spread over 4 or 8 batchers
+                   (as many streams), that many in flight: the host stages batch b + 1 while the
+                   GPU runs batch b, and one batch's tail overlaps the next ones.
     Reported: queries/s over the stream and per-request latency (p50 / p99, from the start of the
     call that serves the request to its results on the host). Every request's rows are checked
     against the plain search on a sample."""
@@ -607,13 +607,13 @@ def study_uneven(args, v, torch):
     total_q = int(offs[-1])
     log(f"uneven stream: {len(requests)} requests, {total_q} queries")
 
-    bts = [v.Batcher(ix, max_queries=4096, max_k=100, max_ef=4 * 100 + 256) for _ in range(4)]
+    bts = [v.Batcher(ix, max_queries=4096, max_k=100, max_ef=4 * 100 + 256) for _ in range(8)]
     bt = bts[0]
 
-    def pack(reqs):
+    def pack(reqs, limit=4096):
         batches, cur, cur_n = [], [], 0
         for i, (q, _, _) in enumerate(reqs):
-            if cur and cur_n + len(q) > 4096:
+            if cur and cur_n + len(q) > limit:
                 batches.append(cur)
                 cur, cur_n = [], 0
             cur.append(i)
@@ -623,6 +623,7 @@ def study_uneven(args, v, torch):
         return batches
 
     batches = pack(requests)
+    batches_1024 = pack(requests, 1024)
     sample = batches[len(batches) // 2]
     sq = np.concatenate([requests[i][0] for i in sample])
     sk = np.concatenate([np.full(len(requests[i][0]), requests[i][1], np.uint32) for i in sample])
@@ -647,7 +648,7 @@ def study_uneven(args, v, torch):
         if not (np.array_equal(a[:, :k], wa) and np.array_equal(b[:, :k], wb) and np.array_equal(c, wc)):
             mismatches += 1
 
-    def serve(mode):
+    def serve(mode, depth=4, packs=None):
         lat = np.zeros(len(requests))
         torch.cuda.synchronize()
         t_all = time.perf_counter()
@@ -662,9 +663,9 @@ def study_uneven(args, v, torch):
                 bt.run(*packed(b))
                 lat[b] = time.perf_counter() - t0
         elif mode == "pipelined":
-            pending = [None] * len(bts)
-            for n_b, b in enumerate(batches):
-                slot = n_b % len(bts)
+            pending = [None] * depth
+            for n_b, b in enumerate(packs):
+                slot = n_b % depth
                 if pending[slot] is not None:
                     bts[slot].wait()
                     lat[pending[slot][0]] = time.perf_counter() - pending[slot][1]
@@ -690,9 +691,13 @@ def study_uneven(args, v, torch):
 
     out = {}
     with Clocks(0) as clocks:
-        for mode in ("per_request", "batcher", "packed", "pipelined"):
+        for mode in ("per_request", "batcher", "packed"):
             serve(mode)  # warm-up pass
             out[mode] = serve(mode)
+        for depth, packs, name in ((4, batches, "pipelined_4x4096"), (8, batches, "pipelined_8x4096"),
+                                   (8, batches_1024, "pipelined_8x1024")):
+            serve("pipelined", depth, packs)
+            out[name] = serve("pipelined", depth, packs)
     line = {"study": "uneven", "workload": f"{n} x 96 IP, 4,096 clusters (log-normal scales), "
                                            f"M24 efc{EF_CONSTRUCTION}; 5,000 requests (seed 51)",
             "queries": total_q, "batches_packed": len(batches), "modes": out,

@@ -41,7 +41,7 @@ constexpr int kBM = 128;                        // queries per tile (MMA M, TMEM
 constexpr int kBN = 128;                        // stored rows per tile (MMA N, TMEM columns)
 constexpr int kBK = 64;                         // K elements per 128-byte swizzled chunk
 constexpr std::uint32_t kChunk = kBM * kBK * 2;  // 16 KB: one 128 x 64 bf16 chunk
-constexpr int kThreads = 256;
+constexpr int kThreads = 384;  // 4 role warps + up to 8 epilogue warps
 constexpr std::uint64_t kWaitNs = 1000000000ull;
 constexpr std::uint32_t kTmemCols = 2 * kBN;   // two accumulator buffers
 
@@ -178,13 +178,14 @@ __device__ __forceinline__ float key_to_float(std::uint32_t k) {
 
 struct TcParams {
     std::uint32_t nq, n, dim, kchunks, qtiles, nchunks, chunk_rows, kc, stages, metric;
+    std::uint32_t halves;                 // epilogue warps per TMEM lane quarter (column halves)
     std::uint32_t base_lo;                // the stored vectors have nonzero lo parts
     const std::uint32_t* query_flags;     // bit 0: some query has a nonzero lo part
     const float* qnorm;                   // [nq]
     const float* xnorm;                   // [n rounded up to a tile]: the score bias
-    std::uint32_t* cand_ids;              // [nq][nchunks][kc]
+    std::uint32_t* cand_ids;              // [nq][nchunks * halves][kc]
     float* cand_d;
-    float* cand_tau;                      // [nq][nchunks]
+    float* cand_tau;                      // [nq][nchunks * halves]
     std::uint32_t* floor_key;             // [nq] best kc-th score of any finished chunk (ordered key)
     std::uint32_t* error;                 // status word: 5 on a timeout
     std::uint32_t off_b, off_lists, off_bar;  // smem offsets from the 1024-aligned base
@@ -208,8 +209,6 @@ __global__ void __launch_bounds__(kThreads, 1)
     const std::uint32_t a_lo = base_addr + p.kchunks * kChunk;
     const std::uint32_t stage_bytes = (xlo ? 2u : 1u) * p.kchunks * kChunk;
     const std::uint32_t b0 = base_addr + p.off_b;
-    float* list_d = reinterpret_cast<float*>(base + p.off_lists);          // [kc][128]
-    std::uint32_t* list_i = reinterpret_cast<std::uint32_t*>(base + p.off_lists + p.kc * kBM * 4);
     const std::uint32_t bar = base_addr + p.off_bar;
     const auto full = [&](std::uint32_t s) { return bar + 8 * s; };
     const auto empty = [&](std::uint32_t s) { return bar + 8 * (S + s); };
@@ -230,8 +229,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         mbar_init(a_empty, 1);
         mbar_init(tfull0, 1);
         mbar_init(tfull0 + 8, 1);
-        mbar_init(tempty0, kBM);
-        mbar_init(tempty0 + 8, kBM);
+        mbar_init(tempty0, kBM * p.halves);
+        mbar_init(tempty0 + 8, kBM * p.halves);
         mbar_init(drain, 1);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -360,13 +359,22 @@ __global__ void __launch_bounds__(kThreads, 1)
         const std::uint64_t t0 = now_ns();
         while (!mbar_try(drain, 0) && now_ns() - t0 < kWaitNs) {
         }
-    } else if (warp >= 4) {
-        // Epilogue: thread e owns query row e of the tile (TMEM lane e). It works in score space,
+    } else if (warp >= 4 && static_cast<std::uint32_t>(warp - 4) < 4 * p.halves) {
+        // Epilogue: thread e owns query row e of the tile (TMEM lane e) in column half `half`
+        // of every tile (with halves = 2, two warps per TMEM lane quarter split the 128 columns,
+        // so two warps per scheduler hide each other's latency), with its own candidate list
+        // (the merge treats each half's list like a chunk of its own). It works in score space,
         // t = 2 q.x - ||x||^2 (L2) or t = q.x (inner product), larger is closer; the per-row
         // offset (-||x||^2, or -0; -inf for padding rows) is read 32 at a time with broadcast
         // 16-byte loads, and a group of 32 scores enters the insertion path only if its best
         // score can beat the list's current worst.
-        const std::uint32_t e = threadIdx.x - 128;
+        const std::uint32_t e = static_cast<std::uint32_t>((warp & 3) * 32 + lane);
+        const std::uint32_t half = static_cast<std::uint32_t>(warp - 4) >> 2;
+        const std::uint32_t groups = (kBN / 32) / p.halves;  // 32-column groups per half
+        const std::uint32_t lists = p.nchunks * p.halves;
+        float* list_d = reinterpret_cast<float*>(base + p.off_lists + half * p.kc * kBM * 8);  // [kc][128]
+        std::uint32_t* list_i = reinterpret_cast<std::uint32_t*>(base + p.off_lists + half * p.kc * kBM * 8 +
+                                                                 p.kc * kBM * 4);
         const std::uint32_t lane_base = static_cast<std::uint32_t>((warp & 3) * 32) << 16;
         const bool l2 = p.metric == 0;
         const float c2 = l2 ? 2.0F : 1.0F;
@@ -394,10 +402,10 @@ __global__ void __launch_bounds__(kThreads, 1)
                     break;
                 }
                 tc_fence_after();
-                for (std::uint32_t cc = 0; cc < kBN / 32; ++cc) {
+                for (std::uint32_t cc = half * groups; cc < (half + 1) * groups; ++cc) {
                     std::uint32_t r[32];
                     tmem_ld32(tmem + lane_base + b * kBN + cc * 32, r);
-                    if (cc == kBN / 32 - 1) {
+                    if (cc == (half + 1) * groups - 1) {
                         tc_fence_before();
                         mbar_arrive(tempty0 + 8 * b);
                     }
@@ -469,7 +477,8 @@ __global__ void __launch_bounds__(kThreads, 1)
             if (live) {
                 // Back to distances: d = ||q||^2 - t (L2) or 1 - t; order is preserved.
                 const float qn = p.qnorm[row];
-                const std::size_t at = (static_cast<std::size_t>(row) * p.nchunks + ch) * p.kc;
+                const std::size_t list = static_cast<std::size_t>(row) * lists + ch * p.halves + half;
+                const std::size_t at = list * p.kc;
                 for (std::uint32_t i = 0; i < p.kc; ++i) {
                     const float v = list_d[i * kBM + e];
                     p.cand_d[at + i] = i < count ? (l2 ? __fsub_rn(qn, v) : __fsub_rn(1.0F, v)) : INFINITY;
@@ -478,7 +487,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                 // Every excluded row of this chunk scored at most `thr` (the floor, or the full
                 // list's kc-th): no excluded distance is below the matching distance.
                 const float bound = count == p.kc ? fmaxf(thr, floor) : floor;
-                p.cand_tau[static_cast<std::size_t>(row) * p.nchunks + ch] =
+                p.cand_tau[list] =
                     bound == -INFINITY ? INFINITY : (l2 ? __fsub_rn(qn, bound) : __fsub_rn(1.0F, bound));
                 if (count == p.kc) {
                     atomicMax(p.floor_key + row, float_to_key(list_d[(p.kc - 1) * kBM + e]));
@@ -768,7 +777,7 @@ bool make_map(CUtensorMap* map, const void* ptr, std::uint32_t rows, std::uint32
 std::size_t align_up(std::size_t x, std::size_t a) { return (x + a - 1) / a * a; }
 
 struct Plan {
-    std::uint32_t dk, kchunks, kc, stages, qtiles, nchunks, chunk_rows;
+    std::uint32_t dk, kchunks, kc, stages, qtiles, nchunks, chunk_rows, halves;
     std::uint32_t off_b, off_lists, off_bar;
     std::size_t smem;
     bool ok;
@@ -786,13 +795,22 @@ Plan make_plan(std::uint32_t nq, std::uint32_t n, std::uint32_t dim, std::uint32
     }
     const std::size_t a_bytes = 2 * pl.kchunks * kChunk;
     const std::size_t stage = (xlo ? 2 : 1) * pl.kchunks * kChunk;
-    const std::size_t lists = static_cast<std::size_t>(pl.kc) * kBM * 8;
     const std::size_t limit = 227 * 1024 - 1024 - 256;
-    std::uint32_t stages = 4;
-    while (stages > 1 && a_bytes + stages * stage + lists > limit) {
-        --stages;
+    // Two epilogue halves (two candidate lists per row) when they fit beside at least two
+    // pipeline stages; otherwise one.
+    std::uint32_t stages = 0;
+    std::size_t lists = 0;
+    for (pl.halves = 2; pl.halves >= 1; --pl.halves) {
+        lists = static_cast<std::size_t>(pl.halves) * pl.kc * kBM * 8;
+        stages = 4;
+        while (stages > 1 && a_bytes + stages * stage + lists > limit) {
+            --stages;
+        }
+        if (a_bytes + stages * stage + lists <= limit && stages >= 2) {
+            break;
+        }
     }
-    if (a_bytes + stages * stage + lists > limit || stages < 2) {
+    if (pl.halves == 0) {
         pl.ok = false;
         return pl;
     }
@@ -897,7 +915,7 @@ std::size_t bruteforce_tc_workspace(std::uint32_t nq, std::uint32_t n, std::uint
     cudaGetDevice(&device);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     const Plan pl = make_plan(nq, n, dim, k, true, sms);
-    const std::size_t chunks = pl.ok ? pl.nchunks : 1;
+    const std::size_t chunks = pl.ok ? static_cast<std::size_t>(pl.nchunks) * pl.halves : 1;
     const std::size_t kc = pl.ok ? pl.kc : 32;
     return 4 * nqp * dk                         // q hi + lo
            + 4 * nqp * row32                    // normalized FP32 queries
@@ -933,9 +951,10 @@ cudaError_t launch_bruteforce_tc(const BruteArgs& a, const TcBase& b, void* work
     auto* qnorm = reinterpret_cast<float*>(take(nqp * 4));
     auto* q_exact = take(nqp);
     auto* q_valid = take(nqp);
-    auto* cand_ids = reinterpret_cast<std::uint32_t*>(take(static_cast<std::size_t>(nq) * pl.nchunks * pl.kc * 4));
-    auto* cand_d = reinterpret_cast<float*>(take(static_cast<std::size_t>(nq) * pl.nchunks * pl.kc * 4));
-    auto* cand_tau = reinterpret_cast<float*>(take(static_cast<std::size_t>(nq) * pl.nchunks * 4));
+    const std::size_t lists = static_cast<std::size_t>(pl.nchunks) * pl.halves;
+    auto* cand_ids = reinterpret_cast<std::uint32_t*>(take(static_cast<std::size_t>(nq) * lists * pl.kc * 4));
+    auto* cand_d = reinterpret_cast<float*>(take(static_cast<std::size_t>(nq) * lists * pl.kc * 4));
+    auto* cand_tau = reinterpret_cast<float*>(take(static_cast<std::size_t>(nq) * lists * 4));
     auto* uncert = reinterpret_cast<std::uint32_t*>(take(nqp * 4));
     auto* floor_key = reinterpret_cast<std::uint32_t*>(take(nqp * 4));
     auto* flags = reinterpret_cast<std::uint32_t*>(take(64));  // [0] query flags [1] max norm [2] error
@@ -981,6 +1000,7 @@ cudaError_t launch_bruteforce_tc(const BruteArgs& a, const TcBase& b, void* work
     p.kchunks = pl.kchunks;
     p.qtiles = pl.qtiles;
     p.nchunks = pl.nchunks;
+    p.halves = pl.halves;
     p.chunk_rows = pl.chunk_rows;
     p.kc = pl.kc;
     p.stages = pl.stages;
@@ -1014,7 +1034,7 @@ cudaError_t launch_bruteforce_tc(const BruteArgs& a, const TcBase& b, void* work
     m.n = n;
     m.dim = dim;
     m.row32 = row32;
-    m.nchunks = pl.nchunks;
+    m.nchunks = static_cast<std::uint32_t>(lists);  // candidate lists per query
     m.kc = pl.kc;
     m.k = a.k;
     m.out_stride = a.out_stride;
