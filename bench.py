@@ -703,7 +703,7 @@ def study_uneven(args, v, torch):
             "queries": total_q, "batches_packed": len(batches), "modes": out,
             "autotune_seconds": round(tune_s, 2),
             "plans": {str(k_): {f: c[f] for f in ("warps_per_block", "rows_per_round", "hash_slots",
-                                                   "result_capacity", "ms")}
+                                                   "global_slots", "result_capacity", "ms")}
                       for k_, c in sorted(chosen.items())},
             "parity_sampled_requests": len(range(0, len(requests), 50)),
             "parity_mismatches": mismatches, "clocks": clocks.summary()}

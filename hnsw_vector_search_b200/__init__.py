@@ -40,7 +40,7 @@ class _IndexInfo(ctypes.Structure):
 
 class _PlanTiming(ctypes.Structure):
     _fields_ = [("ef_class", _U32), ("warps_per_block", _I32), ("rows_per_round", _U32), ("hash_slots", _U32),
-                ("result_capacity", _U32), ("ms", _F)]
+                ("result_capacity", _U32), ("ms", _F), ("global_slots", _U32)]
 
 
 class _GraphReport(ctypes.Structure):

@@ -85,7 +85,7 @@ Batcher::Batcher(const HnswIndex& idx, int dev, Precision prec, std::uint32_t ma
     for (std::size_t i = 0; i < caps.size(); ++i) {
         EfClass& c = classes[i];
         c.cap = caps[i];
-        c.plan = default_plan(graph_view, c.cap);
+        c.plan = default_plan(graph_view, c.cap, true);
         gpu::check(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking), "stream");
         gpu::check(cudaEventCreateWithFlags(&joins[i], cudaEventDisableTiming), "event");
         c.d_queries = dalloc<float>(rows_q, "batch queries");
@@ -129,7 +129,7 @@ Batcher::~Batcher() {
         for (void* p : {static_cast<void*>(c.d_queries), static_cast<void*>(c.d_k),
                         static_cast<void*>(c.d_ef), static_cast<void*>(c.d_nq),
                         static_cast<void*>(c.d_ids), static_cast<void*>(c.d_dists),
-                        static_cast<void*>(c.d_counts), static_cast<void*>(c.d_work)}) {
+                        static_cast<void*>(c.d_counts), static_cast<void*>(c.d_work), c.d_visited}) {
             cudaFree(p);
         }
         for (void* p : {static_cast<void*>(c.h_queries), static_cast<void*>(c.h_k),
@@ -153,7 +153,31 @@ Batcher::~Batcher() {
     cudaSetDevice(prev);
 }
 
-SearchArgs Batcher::args(const EfClass& c) const {
+// Lays out the class's global visited tables for `plan` (grow-only: a larger stride or more
+// warps re-lays them out and zeroes them, so each warp keeps its table and epoch counter).
+void Batcher::bind_visited(EfClass& c, const SearchPlan& plan) {
+    if (plan.global_slots == 0) {
+        return;
+    }
+    SearchArgs probe = args(c, SearchPlan{});
+    const std::uint32_t warps = search_warps(probe, plan);
+    if (c.d_visited == nullptr || plan.global_slots > c.visited_stride || warps > c.visited_warps) {
+        const std::uint32_t stride = std::max(plan.global_slots, c.visited_stride);
+        const std::uint32_t count = std::max(warps, c.visited_warps);
+        const std::size_t bytes = global_visited_bytes(stride, count);
+        if (c.d_visited != nullptr) {
+            gpu::check(cudaDeviceSynchronize(), "visited tables");
+            cudaFree(c.d_visited);
+            c.d_visited = nullptr;
+        }
+        c.d_visited = gpu::device_alloc(bytes, "visited tables");
+        gpu::check(cudaMemset(c.d_visited, 0, bytes), "clear visited tables");
+        c.visited_stride = stride;
+        c.visited_warps = count;
+    }
+}
+
+SearchArgs Batcher::args(const EfClass& c, const SearchPlan& plan) {
     SearchArgs a;
     a.g = graph_view;
     a.queries = c.d_queries;
@@ -176,13 +200,16 @@ SearchArgs Batcher::args(const EfClass& c) const {
         a.rerank = kRerankPerK * max_k;
         a.rerank_per_k = kRerankPerK;
     }
+    if (plan.global_slots > 0 && c.d_visited != nullptr) {
+        bind_global_visited(a, plan, c.d_visited, c.visited_stride, c.visited_warps);
+    }
     return a;
 }
 
-void Batcher::enqueue(const EfClass& c, const SearchPlan& p, cudaStream_t s) {
+void Batcher::enqueue(EfClass& c, const SearchPlan& p, cudaStream_t s) {
     gpu::check(cudaMemsetAsync(c.d_work, 0, kWorkWords * 4, s), "reset work words");
     gpu::check(cudaMemsetAsync(c.d_work + 1, 0xFF, 4, s), "reset work words");
-    SearchArgs a = args(c);
+    SearchArgs a = args(c, p);
     gpu::check(launch_search(a, p, s), "search kernel");
 }
 
@@ -195,6 +222,9 @@ void Batcher::capture() {
     if (graph != nullptr) {
         cudaGraphDestroy(graph);
         graph = nullptr;
+    }
+    for (EfClass& c : classes) {
+        bind_visited(c, c.plan);  // allocation and clearing stay outside the capture
     }
     gpu::check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture");
     gpu::check(cudaEventRecord(fork, stream), "fork");
@@ -310,7 +340,8 @@ void Batcher::run(const float* queries, std::uint32_t nq, const std::uint32_t* k
     wait(ids, dists, counts);
 }
 
-float Batcher::time_plan(const EfClass& c, const SearchPlan& p, int reps) {
+float Batcher::time_plan(EfClass& c, const SearchPlan& p, int reps) {
+    bind_visited(c, p);
     cudaEvent_t a, b;
     gpu::check(cudaEventCreate(&a), "event");
     gpu::check(cudaEventCreate(&b), "event");
@@ -343,28 +374,37 @@ std::vector<TunedPlan> Batcher::autotune(const float* queries, std::uint32_t nq,
         if (c.rows.empty()) {
             continue;
         }
-        const SearchPlan base = default_plan(graph_view, c.cap);
-        SearchPlan best = base;
+        // The visited-filter kind stays the default one (a global table from capacity 512): timed
+        // alone, one batch is a little faster with the shared-memory table, but with batches in
+        // flight on several batchers the global table's smaller per-warp footprint lets their
+        // kernels share the SMs (2.3x the stream throughput on the uneven-stream workload).
+        const std::vector<SearchPlan> bases{default_plan(graph_view, c.cap, true)};
+        SearchPlan best = c.plan;
         float best_ms = -1.0F;
-        for (const int warps : {2, 4, 8}) {
-            for (const std::uint32_t rows : {8u, 16u, 32u}) {
-                for (const std::uint32_t slots : {base.hash_slots / 2, base.hash_slots, base.hash_slots * 2}) {
-                    if (slots < 512) {
-                        continue;
-                    }
-                    SearchPlan p = base;
-                    p.warps_per_block = warps;
-                    p.rows_cap = std::max<std::uint32_t>(1, std::min(rows, graph_view.cap0));
-                    p.hash_slots = slots;
-                    SearchArgs a = args(c);
-                    if (plan_search(a, p) > 200 * 1024) {
-                        continue;
-                    }
-                    const float ms = time_plan(c, p, 3);
-                    tried.push_back({c.cap, p, ms});
-                    if (best_ms < 0.0F || ms < best_ms) {
-                        best_ms = ms;
-                        best = p;
+        for (const SearchPlan& base : bases) {
+            const bool global = base.global_slots > 0;
+            for (const int warps : {2, 4, 8}) {
+                for (const std::uint32_t rows : {8u, 16u, 32u}) {
+                    // Visited-filter size: shared-memory slots, or global slots for large ef.
+                    const std::uint32_t mid = global ? base.global_slots : base.hash_slots;
+                    for (const std::uint32_t slots : {mid / 2, mid, mid * 2}) {
+                        if (slots < 512) {
+                            continue;
+                        }
+                        SearchPlan p = base;
+                        p.warps_per_block = warps;
+                        p.rows_cap = std::max<std::uint32_t>(1, std::min(rows, graph_view.cap0));
+                        (global ? p.global_slots : p.hash_slots) = slots;
+                        SearchArgs a = args(c, p);
+                        if (plan_search(a, p) > 200 * 1024) {
+                            continue;
+                        }
+                        const float ms = time_plan(c, p, 3);
+                        tried.push_back({c.cap, p, ms});
+                        if (best_ms < 0.0F || ms < best_ms) {
+                            best_ms = ms;
+                            best = p;
+                        }
                     }
                 }
             }

@@ -34,6 +34,9 @@ struct EfClass {
                   *h_counts = nullptr, *h_work = nullptr;
     float* h_dists = nullptr;
     std::vector<std::uint32_t> rows;      // batch row of each staged position
+    void* d_visited = nullptr;            // global visited tables (large-ef plans), grow-only
+    std::uint32_t visited_stride = 0;
+    std::uint32_t visited_warps = 0;
 };
 
 struct Batcher {
@@ -72,11 +75,12 @@ struct Batcher {
     cudaGraphExec_t exec = nullptr;
 
 private:
-    SearchArgs args(const EfClass& c) const;
-    void enqueue(const EfClass& c, const SearchPlan& plan, cudaStream_t stream);
+    SearchArgs args(const EfClass& c, const SearchPlan& plan);
+    void bind_visited(EfClass& c, const SearchPlan& plan);
+    void enqueue(EfClass& c, const SearchPlan& plan, cudaStream_t stream);
     void capture();
     void stage(const float* queries, std::uint32_t nq, const std::uint32_t* k, const std::uint32_t* ef);
-    float time_plan(const EfClass& c, const SearchPlan& plan, int reps);
+    float time_plan(EfClass& c, const SearchPlan& plan, int reps);
 };
 
 }  // namespace vdx::dev

@@ -356,8 +356,10 @@ vdx_status vdx_batcher_autotune(vdx_batcher* batcher, const float* queries, uint
         check_batch_size(*batcher, nq);
         const auto tried = batcher->b.autotune(queries, static_cast<uint32_t>(nq), k_per_q, ef_per_q);
         for (std::size_t i = 0; i < tried.size() && i < cap; ++i) {
-            timings[i] = {tried[i].ef_class, tried[i].plan.warps_per_block, tried[i].plan.rows_cap,
-                          tried[i].plan.hash_slots, tried[i].plan.efcap, tried[i].ms};
+            const vdx::dev::SearchPlan& pl = tried[i].plan;
+            timings[i] = {tried[i].ef_class, pl.warps_per_block, pl.rows_cap,
+                          pl.global_slots > 0 ? 0u : pl.hash_slots, pl.efcap, tried[i].ms,
+                          pl.global_slots};
         }
         if (n_out != nullptr) {
             *n_out = tried.size();

@@ -112,7 +112,7 @@ Workspace::~Workspace() {
     cudaGetDevice(&prev);
     cudaSetDevice(device);
     for (void* p : {static_cast<void*>(queries), static_cast<void*>(ids), static_cast<void*>(dists),
-                    static_cast<void*>(counts), static_cast<void*>(small), scratch}) {
+                    static_cast<void*>(counts), static_cast<void*>(small), scratch, visited}) {
         if (p != nullptr) {
             cudaFree(p);
         }
@@ -153,6 +153,24 @@ void* Workspace::scratch_bytes(std::size_t bytes) {
         scratch_cap = bytes;
     }
     return scratch;
+}
+
+void* Workspace::visited_for(std::uint32_t slots, std::uint32_t warps) {
+    if (visited == nullptr || slots > visited_stride || warps > visited_warps) {
+        const std::uint32_t stride = std::max(slots, visited_stride);
+        const std::uint32_t count = std::max(warps, visited_warps);
+        const std::size_t bytes = dev::global_visited_bytes(stride, count);
+        if (visited != nullptr) {
+            check(cudaStreamSynchronize(stream), "visited tables");
+            cudaFree(visited);
+            visited = nullptr;
+        }
+        visited = device_alloc(bytes, "visited tables");
+        check(cudaMemsetAsync(visited, 0, bytes, stream), "clear visited tables");
+        visited_stride = stride;
+        visited_warps = count;
+    }
+    return visited;
 }
 
 // Resets the status words (code 0, first bad row UINT32_MAX), the claim counter and the stats.
@@ -488,7 +506,12 @@ void HnswIndex::search_batch_into(MatrixView<float> queries, std::size_t k, std:
         a.stop_threshold = options.stop_threshold;
     }
     const std::size_t ef_eff = std::min<std::size_t>(std::max(ef, k), size());
-    dev::SearchPlan plan = dev::default_plan(dg.view, static_cast<std::uint32_t>(ef_eff));
+    dev::SearchPlan plan = dev::default_plan(dg.view, static_cast<std::uint32_t>(ef_eff), true);
+    if (plan.global_slots > 0) {
+        const std::uint32_t warps = dev::search_warps(a, plan);
+        void* buf = ws.visited_for(plan.global_slots, warps);
+        dev::bind_global_visited(a, plan, buf, ws.visited_stride, ws.visited_warps);
+    }
     gpu::check(dev::launch_search(a, plan, ws.stream), "search kernel");
     gpu::check(cudaMemcpyAsync(ws.small_host, ws.small, 256, cudaMemcpyDeviceToHost, ws.stream),
                "copy status");

@@ -35,6 +35,9 @@ struct Workspace {
     std::uint32_t* small_host = nullptr;
     void* scratch = nullptr;
     std::size_t scratch_cap = 0;
+    void* visited = nullptr;          // global visited tables of large-ef searches
+    std::uint32_t visited_stride = 0; // slots per warp's table
+    std::uint32_t visited_warps = 0;  // warps laid out
     unsigned long long last_stats[16] = {};
 
     Workspace() = default;
@@ -43,6 +46,10 @@ struct Workspace {
     ~Workspace();
     void reserve(std::size_t nq, std::size_t dim, std::size_t width);
     void* scratch_bytes(std::size_t bytes);
+    // Global visited tables for `warps` warps of at least `slots` slots each. The layout only
+    // grows (a larger stride or more warps re-lays it out and zeroes it on this workspace's
+    // stream), so each warp's table and epoch counter keep their place between launches.
+    void* visited_for(std::uint32_t slots, std::uint32_t warps);
 };
 
 void check(cudaError_t err, const char* what);

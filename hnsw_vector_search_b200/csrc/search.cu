@@ -70,6 +70,33 @@ __device__ __forceinline__ bool first_visit(std::uint32_t* table, std::uint32_t 
     return true;
 }
 
+// The same filter in global memory, for large ef (a per-warp table too big for shared memory):
+// 64-bit slots hold (query epoch << 32 | id); a slot whose epoch is not the current query's is
+// empty, so the table never needs clearing between queries. Only this warp's lanes write its
+// table, so a claim can be lost only to a lane of the same warp writing the current epoch, which
+// ends the inner loop: every loop is bounded.
+__device__ __forceinline__ bool first_visit_global(unsigned long long* table, std::uint32_t mask,
+                                                   std::uint32_t id, std::uint32_t epoch) {
+    const unsigned long long key = (static_cast<unsigned long long>(epoch) << 32) | id;
+    std::uint32_t h = (id * 2654435761u) & mask;
+#pragma unroll 1
+    for (int p = 0; p < kProbes; ++p) {
+        unsigned long long old = __ldcg(table + h);
+        while (static_cast<std::uint32_t>(old >> 32) != epoch) {
+            const unsigned long long prev = atomicCAS(table + h, old, key);
+            if (prev == old) {
+                return true;
+            }
+            old = prev;
+        }
+        if (old == key) {
+            return false;
+        }
+        h = (h + 1) & mask;
+    }
+    return true;
+}
+
 // Copies `count` rows (ids in `ids`, shared) of `row_bytes` each from `base` into `dst`
 // (shared, rows `dst_stride` bytes apart), 16 bytes per lane per step, and commits them as one
 // cp.async group. `shift` is log2(row_bytes / 16) when that is a power of two up to 32 (several
@@ -249,6 +276,15 @@ __global__ void __launch_bounds__(256) search_kernel(const SearchArgs a) {
     // A device-side batch size never exceeds the buffers' capacity (a.nq).
     const std::uint32_t nq = a.nq_device != nullptr ? min(*a.nq_device, a.nq) : a.nq;
     const std::uint32_t hmask = a.hash_slots - 1;
+    // With a global visited filter each warp of the grid owns one table and one epoch counter.
+    const std::uint32_t gwarp = blockIdx.x * (blockDim.x >> 5) + static_cast<std::uint32_t>(warp);
+    unsigned long long* const gtable =
+        a.gvisited != nullptr ? a.gvisited + static_cast<std::size_t>(gwarp) * a.gstride : nullptr;
+    const std::uint32_t gmask = a.gslots - 1;
+    const auto visit = [&](std::uint32_t id, std::uint32_t epoch) {
+        return gtable != nullptr ? first_visit_global(gtable, gmask, id, epoch)
+                                 : first_visit(table, hmask, id);
+    };
     // Two lanes score each row (pair_distance), so a round stages at most 16 rows.
     const int rounds_cap = static_cast<int>(a.rows_cap < 16 ? a.rows_cap : 16);
     const std::uint32_t stride_s = padded_row_stride(g.row_bytes);
@@ -415,12 +451,32 @@ __global__ void __launch_bounds__(256) search_kernel(const SearchArgs a) {
         }
 
         // 3. Layer-0 beam.
-        for (std::uint32_t i = lane; i < a.hash_slots; i += 32) {
-            table[i] = kNoId;
+        std::uint32_t epoch = 0;
+        if (gtable != nullptr) {
+            if (lane == 0) {
+                epoch = a.gepoch[gwarp] + 1;
+                a.gepoch[gwarp] = epoch;
+            }
+            epoch = __shfl_sync(kFull, epoch, 0);
+            if (epoch == 0xFFFFFFFFu) {
+                // Epochs wrapped (after 2^32 queries on this warp): clear and restart at 1.
+                for (std::uint32_t i = lane; i < a.gstride; i += 32) {
+                    gtable[i] = 0;
+                }
+                __syncwarp();
+                epoch = 1;
+                if (lane == 0) {
+                    a.gepoch[gwarp] = 1;
+                }
+            }
+        } else {
+            for (std::uint32_t i = lane; i < a.hash_slots; i += 32) {
+                table[i] = kNoId;
+            }
         }
         __syncwarp();
         if (lane == 0) {
-            first_visit(table, hmask, cur);
+            visit(cur, epoch);
             rd[0] = curd;
             rid[0] = cur;
         }
@@ -485,7 +541,7 @@ __global__ void __launch_bounds__(256) search_kernel(const SearchArgs a) {
                 }
                 const bool present = id != kNoId;
                 count += __popc(__ballot_sync(kFull, present));
-                const bool isnew = present && first_visit(table, hmask, id);
+                const bool isnew = present && visit(id, epoch);
                 const std::uint32_t m = __ballot_sync(kFull, isnew);
                 if (isnew) {
                     fresh[f + __popc(m & ((1u << lane) - 1u))] = id;
@@ -691,6 +747,16 @@ cudaError_t launch_typed(SearchArgs& args, const SearchPlan& plan, std::size_t s
     if (args.nq_device == nullptr && static_cast<std::uint32_t>(blocks) > needed) {
         blocks = static_cast<int>(needed > 0 ? needed : 1);
     }
+    if (plan.global_slots > 0) {
+        // One table per warp of the grid: the caller's buffer must hold them all.
+        if (args.gvisited == nullptr || args.gepoch == nullptr || args.gslots != plan.global_slots ||
+            args.gstride < args.gslots ||
+            static_cast<std::uint64_t>(blocks) * plan.warps_per_block > args.gwarps) {
+            return cudaErrorInvalidValue;
+        }
+    } else {
+        args.gvisited = nullptr;
+    }
     kernel<<<blocks, threads, smem, stream>>>(args);
     return cudaGetLastError();
 }
@@ -700,13 +766,13 @@ cudaError_t launch_typed(SearchArgs& args, const SearchPlan& plan, std::size_t s
 std::size_t plan_search(SearchArgs& a, const SearchPlan& plan) {
     const DeviceGraphView& g = a.g;
     a.efcap = plan.efcap;
-    a.hash_slots = plan.hash_slots;
+    a.hash_slots = plan.global_slots > 0 ? 0 : plan.hash_slots;
     a.rows_cap = plan.rows_cap;
     std::uint32_t off = round_up(g.dim, 4) * 4;  // query
     a.off_r = off;
     off += round_up(plan.efcap * 8, 16);
     a.off_hash = off;
-    off += plan.hash_slots * 4;
+    off += a.hash_slots * 4;
     a.off_links = off;
     off += 2 * g.stride0 * 4;
     a.off_rows = off;
@@ -725,7 +791,7 @@ std::size_t plan_search(SearchArgs& a, const SearchPlan& plan) {
     return static_cast<std::size_t>(a.warp_bytes) * plan.warps_per_block;
 }
 
-SearchPlan default_plan(const DeviceGraphView& g, std::uint32_t max_ef) {
+SearchPlan default_plan(const DeviceGraphView& g, std::uint32_t max_ef, bool allow_global) {
     SearchPlan p;
     std::uint32_t cap = 32;
     while (cap < max_ef) {
@@ -742,6 +808,15 @@ SearchPlan default_plan(const DeviceGraphView& g, std::uint32_t max_ef) {
         slots <<= 1;
     }
     p.hash_slots = slots;
+    if (allow_global && cap >= 512) {
+        // A shared-memory table of 16 slots per result entry (32 KB and up) would leave a few
+        // warps per SM; a global table of 32 slots per entry (load <= 0.5) costs an L2 round per
+        // filter instead. Side by side on the 1M x 128 workload the two are within 2 % at
+        // ef = 256 and 512 (the shared table slightly ahead), so the switch is at 512; the
+        // batcher's autotuner tries both from capacity 256.
+        p.global_slots = 32 * cap;
+        slots = 0;
+    }
     // Rows staged per round: 16 keeps the per-warp footprint small enough for 12+ resident
     // warps per SM with FP32 rows; expansions with more unvisited neighbors take two rounds.
     p.rows_cap = g.cap0 < 16 ? (g.cap0 > 0 ? g.cap0 : 1) : 16;
@@ -749,6 +824,62 @@ SearchPlan default_plan(const DeviceGraphView& g, std::uint32_t max_ef) {
                                  p.rows_cap * padded_row_stride(g.row_bytes) + 1024;
     p.warps_per_block = per_warp * 4 <= 200 * 1024 ? 4 : (per_warp * 2 <= 200 * 1024 ? 2 : 1);
     return p;
+}
+
+std::uint32_t search_warps(SearchArgs& args, const SearchPlan& plan) {
+    if (plan.blocks > 0) {
+        return static_cast<std::uint32_t>(plan.blocks * plan.warps_per_block);
+    }
+    const std::size_t smem = plan_search(args, plan);
+    int device = 0;
+    cudaGetDevice(&device);
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    const int threads = plan.warps_per_block * 32;
+    const auto per_sm_of = [&](const void* kernel) {
+        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+        int per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
+        return per_sm > 0 ? per_sm : 1;
+    };
+    const bool l2 = args.g.metric == 0;
+    int per_sm = 1;
+    switch (args.g.precision) {
+        case 0:
+            per_sm = l2 ? per_sm_of(reinterpret_cast<const void*>(&search_kernel<kFP32, true>))
+                        : per_sm_of(reinterpret_cast<const void*>(&search_kernel<kFP32, false>));
+            break;
+        case 1:
+            per_sm = l2 ? per_sm_of(reinterpret_cast<const void*>(&search_kernel<kBF16, true>))
+                        : per_sm_of(reinterpret_cast<const void*>(&search_kernel<kBF16, false>));
+            break;
+        default:
+            per_sm = l2 ? per_sm_of(reinterpret_cast<const void*>(&search_kernel<kFP8, true>))
+                        : per_sm_of(reinterpret_cast<const void*>(&search_kernel<kFP8, false>));
+            break;
+    }
+    return static_cast<std::uint32_t>(sms * per_sm * plan.warps_per_block);
+}
+
+std::size_t global_visited_bytes(std::uint32_t stride, std::uint32_t warps) {
+    if (stride == 0) {
+        return 0;
+    }
+    return static_cast<std::size_t>(round_up(warps * 4, 256)) + static_cast<std::size_t>(warps) * stride * 8;
+}
+
+void bind_global_visited(SearchArgs& args, const SearchPlan& plan, void* buffer, std::uint32_t stride,
+                         std::uint32_t warps) {
+    if (plan.global_slots == 0 || buffer == nullptr) {
+        args.gvisited = nullptr;
+        return;
+    }
+    auto* b = static_cast<unsigned char*>(buffer);
+    args.gepoch = reinterpret_cast<std::uint32_t*>(b);
+    args.gvisited = reinterpret_cast<unsigned long long*>(b + round_up(warps * 4, 256));
+    args.gslots = plan.global_slots;
+    args.gstride = stride;
+    args.gwarps = warps;
 }
 
 cudaError_t launch_search(SearchArgs& args, const SearchPlan& plan, cudaStream_t stream) {

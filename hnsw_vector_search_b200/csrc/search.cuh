@@ -83,6 +83,11 @@ struct SearchArgs {
                                            // largest such width, for the scratch sizing)
     StopNetView stop{};
     const void* stop_enabled = nullptr;    // non-null: learned early termination is on
+    unsigned long long* gvisited = nullptr; // global visited tables, one per warp (or null)
+    std::uint32_t* gepoch = nullptr;        // per-warp query epoch counters
+    std::uint32_t gslots = 0;               // slots a query uses (power of two, <= gstride)
+    std::uint32_t gstride = 0;              // slots between two warps' tables
+    std::uint32_t gwarps = 0;               // warps the tables were sized for
     float stop_threshold = 0.5F;
     std::uint32_t stop_min_hops = 16;
     TraceArgs trace{};
@@ -96,7 +101,9 @@ struct SearchArgs {
 struct SearchPlan {
     int warps_per_block = 4;
     std::uint32_t efcap = 64;        // result-list capacity (>= every effective ef)
-    std::uint32_t hash_slots = 2048; // visited-filter slots (power of two)
+    std::uint32_t hash_slots = 2048; // visited-filter slots in shared memory (power of two)
+    std::uint32_t global_slots = 0;  // > 0: the visited filter is a per-warp global table of
+                                     // this many 8-byte slots (power of two) instead
     std::uint32_t rows_cap = 32;     // rows gathered per round
     int blocks = 0;                  // 0: as many as fit on the device
 };
@@ -104,8 +111,20 @@ struct SearchPlan {
 // Fills the layout fields of `args` for `plan`; returns the dynamic shared memory per block.
 std::size_t plan_search(SearchArgs& args, const SearchPlan& plan);
 
-// The default plan for a graph and the largest effective ef of a batch.
-SearchPlan default_plan(const DeviceGraphView& g, std::uint32_t max_ef);
+// The default plan for a graph and the largest effective ef of a batch. allow_global: the caller
+// can provide global visited tables (global_visited_bytes), used from ef capacity 512 up.
+SearchPlan default_plan(const DeviceGraphView& g, std::uint32_t max_ef, bool allow_global = false);
+
+// Warps the launch of `plan` runs (the grid the launcher picks before trimming it to a short
+// batch), and the bytes of global visited tables and epoch counters for `warps` warps of
+// `stride` slots each. A buffer is zeroed once when laid out; it stays valid for every later
+// launch on one stream whose plan needs at most `stride` slots and `warps` warps (each warp's
+// table and epoch counter keep their place, and epochs only grow).
+std::uint32_t search_warps(SearchArgs& args, const SearchPlan& plan);
+std::size_t global_visited_bytes(std::uint32_t stride, std::uint32_t warps);
+// Points args at a global visited buffer laid out for `warps` warps of `stride` slots.
+void bind_global_visited(SearchArgs& args, const SearchPlan& plan, void* buffer,
+                         std::uint32_t stride, std::uint32_t warps);
 
 // Launches the search for args.nq queries on `stream` (status, claim and stats must be zeroed
 // on that stream first). Returns the CUDA error of the launch.

@@ -160,9 +160,10 @@ typedef struct vdx_plan_timing {
     uint32_t ef_class;          /* the class's largest effective ef */
     int32_t warps_per_block;
     uint32_t rows_per_round;
-    uint32_t hash_slots;
+    uint32_t hash_slots;        /* visited-filter slots in shared memory (0 with a global table) */
     uint32_t result_capacity;
     float ms;
+    uint32_t global_slots;      /* > 0: the visited filter is a global table of this many slots */
 } vdx_plan_timing;
 
 /* A batcher for batches of up to max_queries queries with per-query k <= max_k and

@@ -52,8 +52,9 @@ def small_l2(orc, tmp_path_factory):
     return path, base, queries
 
 
-@pytest.mark.parametrize("ef", [16, 64, 128])
+@pytest.mark.parametrize("ef", [16, 64, 128, 300, 700])
 def test_gpu_equals_reference_on_small_l2(gpu, orc, small_l2, ef):
+    """ef 300 and 700 (result capacity 512 and 1024) run with the global visited filter."""
     path, base, queries = small_l2
     ref = orc.RefHnsw.load(path)
     ix = gpu.HnswIndex.load(path)
