@@ -262,7 +262,7 @@ def main():
                     help="one search launch per warm-up step on the cached workload (for ncu)")
     ap.add_argument("--mode", default="fp32", choices=["fp32", "bf16", "fp8", "bf_tc", "bf_exact"])
     ap.add_argument("--ef", type=int, default=32)
-    ap.add_argument("--study", choices=["uneven", "precision"],
+    ap.add_argument("--study", choices=["uneven", "precision", "build"],
                     help="instead of the headline: the uneven-batch stream or the precision study")
     ap.add_argument("--rows", type=int, default=0, help="base rows of a study (0: its default)")
     args = ap.parse_args()
@@ -296,6 +296,9 @@ def main():
         return
     if args.study == "precision":
         study_precision(args, v, torch)
+        return
+    if args.study == "build":
+        study_build(args, v, torch)
         return
     base, queries = workload()
     cpu = None
@@ -757,6 +760,43 @@ def study_precision(args, v, torch):
     print(json.dumps({"study": "precision", "workload": f"{n} x 100 cosine glove-like, "
                       f"10k queries (2% duplicates), M16 efc{EF_CONSTRUCTION}", "k": K,
                       "table": table}), flush=True)
+
+
+def study_build(args, v, torch):
+    """Graph construction on the headline workload (1M x 128 sift-like, M 16,
+    ef_construction 200): this library's batched GPU build against the reference's parallel
+    build on all host cores, each timed end to end (vectors in host memory to a searchable
+    index), and the recall@10 of the GPU search on each graph at ef 36 and 64."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as o
+    base, queries = workload()
+    truth = ground_truth(base, queries)
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    ref = o.RefHnsw(128, 0, M, EF_CONSTRUCTION, SEED)
+    ref.add(base, threads=0)
+    ref_s = time.perf_counter() - t0
+    tmp = CACHE / "study_build_ref.vdx"
+    ref.save(tmp)
+    del ref
+    ref_ix = v.HnswIndex.load(tmp)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    gpu_ix = v.HnswIndex(128, "l2", M=M, ef_construction=EF_CONSTRUCTION, seed=SEED)
+    gpu_ix.add(base, device=0)
+    torch.cuda.synchronize()
+    gpu_s = time.perf_counter() - t0
+    rep = gpu_ix.inspect()
+    out = {}
+    for name, ix in (("reference_parallel", ref_ix), ("gpu", gpu_ix)):
+        out[name] = {ef: round(recall_at_10(ix.search_batch(queries, K, ef)[0], truth), 4) for ef in (36, 64)}
+    print(json.dumps({"study": "build", "workload": "1M x 128 L2 sift-like, M16 efc200",
+                      "reference_parallel_seconds": round(ref_s, 2), "reference_threads": threads,
+                      "gpu_seconds": round(gpu_s, 2), "speedup": round(ref_s / gpu_s, 2),
+                      "recall_at_10": out,
+                      "gpu_graph": {"violations": rep["violations"], "reachable": rep["reachable"],
+                                    "max_level": rep["max_level"],
+                                    "mean_degree0": round(rep["mean_degree0"], 3)}}), flush=True)
 
 
 def profile(args, v, torch):

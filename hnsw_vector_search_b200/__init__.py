@@ -73,6 +73,7 @@ def lib() -> ctypes.CDLL:
         "vdx_index_free": (None, [_P]),
         "vdx_index_add": (ctypes.c_int, [_P, _P, _U64, _U64, _U64]),
         "vdx_index_add_one": (ctypes.c_int, [_P, _P, _U64, ctypes.POINTER(_U32)]),
+        "vdx_index_add_gpu": (ctypes.c_int, [_P, _P, _U64, _U64, _I32]),
         "vdx_index_save": (ctypes.c_int, [_P, ctypes.c_char_p]),
         "vdx_index_load": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(_P)]),
         "vdx_index_info_get": (ctypes.c_int, [_P, ctypes.POINTER(_IndexInfo)]),
@@ -179,11 +180,16 @@ class HnswIndex:
     def __len__(self) -> int:
         return self.info()["size"]
 
-    def add(self, rows, num_threads: int = 1) -> None:
+    def add(self, rows, num_threads: int = 1, *, device: int | None = None) -> None:
+        """The reference's add (num_threads host threads), or with `device` the batched GPU
+        build (HnswIndex::add_gpu)."""
         d = self.dim
         a = _rows(rows, d)
-        _raise(lib().vdx_index_add(self._h, _ptr(a), a.shape[0], a.shape[1] if a.ndim == 2 else d,
-                                   num_threads))
+        cols = a.shape[1] if a.ndim == 2 else d
+        if device is not None:
+            _raise(lib().vdx_index_add_gpu(self._h, _ptr(a), a.shape[0], cols, int(device)))
+            return
+        _raise(lib().vdx_index_add(self._h, _ptr(a), a.shape[0], cols, num_threads))
 
     def add_one(self, vector) -> int:
         v = np.ascontiguousarray(np.asarray(vector, dtype=np.float32).ravel())

@@ -117,6 +117,17 @@ vdx_status vdx_index_add(vdx_index* index, const float* rows, uint64_t n, uint64
     });
 }
 
+vdx_status vdx_index_add_gpu(vdx_index* index, const float* rows, uint64_t n, uint64_t dim,
+                             int32_t device) {
+    return guarded([&] {
+        require(index, "index");
+        if (n > 0) {
+            require(rows, "rows");
+        }
+        index->index.add_gpu(vdx::MatrixView<float>(std::span<const float>(rows, n * dim), dim), device);
+    });
+}
+
 vdx_status vdx_index_add_one(vdx_index* index, const float* vector, uint64_t dim, uint32_t* id) {
     return guarded([&] {
         require(index, "index");

@@ -105,6 +105,12 @@ public:
     // the reference's, byte for byte once saved).
     Id add(std::span<const float> vector);
     void add(MatrixView<float> vectors, std::size_t num_threads = 1);
+    // The same insertion, batched on the GPU (device `device`): the first 1024 nodes one by one
+    // on the host as the serial build, then batches of up to 8192 nodes searched, linked and
+    // linked back by kernels, with the serial order's levels. The graph is as good as a parallel
+    // build's (recall within 0.005 of the serial build), not the serial graph itself; the FP32
+    // device mirror is built in place.
+    void add_gpu(MatrixView<float> vectors, int device);
     void add(const Matrix<float>& vectors, std::size_t num_threads = 1);
 
     // Up to k nearest neighbors, closest first, ties by smaller id; ef below k is raised to k.
