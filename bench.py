@@ -262,7 +262,7 @@ def main():
                     help="one search launch per warm-up step on the cached workload (for ncu)")
     ap.add_argument("--mode", default="fp32", choices=["fp32", "bf16", "fp8", "bf_tc", "bf_exact"])
     ap.add_argument("--ef", type=int, default=32)
-    ap.add_argument("--study", choices=["uneven", "precision", "build"],
+    ap.add_argument("--study", choices=["uneven", "precision", "build", "device_image"],
                     help="instead of the headline: the uneven-batch stream or the precision study")
     ap.add_argument("--rows", type=int, default=0, help="base rows of a study (0: its default)")
     args = ap.parse_args()
@@ -297,6 +297,8 @@ def main():
     if args.study == "precision":
         study_precision(args, v, torch)
         return
+    if args.study == "device_image":
+        return study_device_image(args, v, torch)
     if args.study == "build":
         study_build(args, v, torch)
         return
@@ -797,6 +799,40 @@ def study_build(args, v, torch):
                       "gpu_graph": {"violations": rep["violations"], "reachable": rep["reachable"],
                                     "max_level": rep["max_level"],
                                     "mean_degree0": round(rep["mean_degree0"], 3)}}), flush=True)
+
+
+def study_device_image(args, v, torch):
+    """Cold start of the headline graph (1M x 128, M 16) on the GPU: the v1 file loaded and its
+    FP32 device mirror uploaded (padding and link repacking on the way), against the same v1
+    load followed by the device-image sidecar, copied section by section. Both files are read
+    from the page cache (written just before); each path is timed twice, best kept."""
+    base, _ = workload()
+    graph = reference_graph(base)
+    image = CACHE / (graph.stem + ".vdxdev")
+    t0 = time.perf_counter()
+    v.HnswIndex.load(graph).save_device_image(image)
+    save_s = time.perf_counter() - t0
+    best = {"upload": [], "sidecar": [], "v1_load": []}
+    for _ in range(2):
+        t0 = time.perf_counter()
+        ix = v.HnswIndex.load(graph)
+        t1 = time.perf_counter()
+        ix.upload(0, "fp32")
+        torch.cuda.synchronize()
+        best["v1_load"].append(t1 - t0)
+        best["upload"].append(time.perf_counter() - t1)
+        del ix
+        ix = v.HnswIndex.load(graph)
+        t1 = time.perf_counter()
+        ix.load_device_image(image, 0)
+        torch.cuda.synchronize()
+        best["sidecar"].append(time.perf_counter() - t1)
+        del ix
+    print(json.dumps({"study": "device_image", "workload": "1M x 128 L2 sift-like, M16",
+                      "image_bytes": image.stat().st_size, "save_seconds": round(save_s, 3),
+                      "v1_load_seconds": round(min(best["v1_load"]), 3),
+                      "upload_seconds": round(min(best["upload"]), 3),
+                      "sidecar_seconds": round(min(best["sidecar"]), 3)}), flush=True)
 
 
 def profile(args, v, torch):

@@ -76,6 +76,9 @@ def lib() -> ctypes.CDLL:
         "vdx_index_add_gpu": (ctypes.c_int, [_P, _P, _U64, _U64, _I32]),
         "vdx_index_save": (ctypes.c_int, [_P, ctypes.c_char_p]),
         "vdx_index_load": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(_P)]),
+        "vdx_index_save_device_image": (ctypes.c_int, [_P, ctypes.c_char_p]),
+        "vdx_index_load_device_image": (ctypes.c_int, [_P, ctypes.c_char_p, _I32]),
+        "vdx_index_graph_hash": (ctypes.c_int, [_P, ctypes.POINTER(_U64)]),
         "vdx_index_info_get": (ctypes.c_int, [_P, ctypes.POINTER(_IndexInfo)]),
         "vdx_index_inspect": (ctypes.c_int, [_P, ctypes.POINTER(_GraphReport), ctypes.c_char_p, _U64]),
         "vdx_search_batch": (ctypes.c_int, [_P, _P, _U64, _U64, _U64, _U64, _P, _P, _P,
@@ -199,6 +202,22 @@ class HnswIndex:
 
     def save(self, path) -> None:
         _raise(lib().vdx_index_save(self._h, os.fsencode(path)))
+
+    def save_device_image(self, path) -> None:
+        """Write the FP32 device mirror as a sidecar file (host only): a 4096-byte header naming
+        this graph by its XXH64, then the device arrays, each section 4096-byte aligned."""
+        _raise(lib().vdx_index_save_device_image(self._h, os.fsencode(path)))
+
+    def load_device_image(self, path, device: int = 0) -> None:
+        """Install a sidecar written by save_device_image as the FP32 mirror on `device`, one
+        copy per section; raises OSError if it belongs to another graph."""
+        _raise(lib().vdx_index_load_device_image(self._h, os.fsencode(path), device))
+
+    def graph_hash(self) -> int:
+        """XXH64 of the vectors, levels, layer-0 and upper blocks (the device image's key)."""
+        out = _U64()
+        _raise(lib().vdx_index_graph_hash(self._h, ctypes.byref(out)))
+        return int(out.value)
 
     @classmethod
     def load(cls, path) -> "HnswIndex":

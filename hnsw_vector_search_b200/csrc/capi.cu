@@ -155,6 +155,30 @@ vdx_status vdx_index_load(const char* path, vdx_index** out) {
     });
 }
 
+vdx_status vdx_index_save_device_image(const vdx_index* index, const char* path) {
+    return guarded([&] {
+        require(index, "index");
+        require(path, "path");
+        index->index.save_device_image(path);
+    });
+}
+
+vdx_status vdx_index_load_device_image(const vdx_index* index, const char* path, int32_t device) {
+    return guarded([&] {
+        require(index, "index");
+        require(path, "path");
+        index->index.load_device_image(path, device);
+    });
+}
+
+vdx_status vdx_index_graph_hash(const vdx_index* index, uint64_t* out) {
+    return guarded([&] {
+        require(index, "index");
+        require(out, "out");
+        *out = index->index.graph_hash();
+    });
+}
+
 vdx_status vdx_index_info_get(const vdx_index* index, vdx_index_info* out) {
     return guarded([&] {
         require(index, "index");

@@ -144,6 +144,17 @@ public:
     // Never uploads, so it never allocates.
     const DeviceGraph* uploaded_graph(int device, Precision precision) const;
 
+    // The FP32 device mirror as a sidecar file beside the v1 index file: the device arrays in
+    // their device layout, each section 4096-byte aligned, behind a 4096-byte header that names
+    // the graph by graph_hash(). save_device_image() runs on the host only;
+    // load_device_image() installs the file as the FP32 mirror for `device` with one copy per
+    // section (no repacking), and throws std::runtime_error if the file belongs to another
+    // graph, is truncated or is not a device image.
+    void save_device_image(const std::filesystem::path& path) const;
+    void load_device_image(const std::filesystem::path& path, int device) const;
+    // XXH64 of the vectors, levels, layer-0 blocks and upper blocks, in that order.
+    std::uint64_t graph_hash() const;
+
     // Learned early termination: the model SearchOptions::learned_stop uses.
     void set_stop_model(StopModel model);
     bool has_stop_model() const noexcept { return !stop_model_.weights.empty(); }

@@ -97,6 +97,18 @@ VDX_API vdx_status vdx_index_add_one(vdx_index* index, const float* vector, uint
 VDX_API vdx_status vdx_index_save(const vdx_index* index, const char* path);
 /* load(path): include/vecdex/hnsw.hpp:123 */
 VDX_API vdx_status vdx_index_load(const char* path, vdx_index** out);
+/* No reference counterpart (the reference has no device mirror). The FP32 device mirror as a
+ * sidecar file next to the v1 index file: a 4096-byte header, then the device arrays (FP32 rows
+ * padded to 16 bytes, layer-0 blocks, upper-block index, upper blocks), each section 4096-byte
+ * aligned. save writes it on the host; load installs it as the FP32 mirror of `device` with one
+ * copy per section and fails (VDX_ERR_IO) if the file names another graph (its XXH64 of the
+ * vectors, levels and link blocks differs), is truncated or is not a device image. */
+VDX_API vdx_status vdx_index_save_device_image(const vdx_index* index, const char* path);
+VDX_API vdx_status vdx_index_load_device_image(const vdx_index* index, const char* path,
+                                               int32_t device);
+/* No reference counterpart: the XXH64 a device image names its graph by (the vectors, the
+ * levels, the layer-0 blocks and the upper blocks of the v1 layout, hashed in that order). */
+VDX_API vdx_status vdx_index_graph_hash(const vdx_index* index, uint64_t* out);
 /* size() / dim() / metric() / params() / memory_bytes(): include/vecdex/hnsw.hpp:74-77,105 */
 VDX_API vdx_status vdx_index_info_get(const vdx_index* index, vdx_index_info* out);
 /* inspect(): include/vecdex/hnsw.hpp:102; the first violation's text is copied into `first`
