@@ -151,6 +151,7 @@ class HnswIndex:
 
     def __init__(self, dim: int, metric: str | int = "l2", M: int = 16,
                  ef_construction: int = 200, seed: int = 42, *, _handle=None):
+        self._dim = None
         if _handle is not None:
             self._h = _handle
             return
@@ -178,7 +179,11 @@ class HnswIndex:
 
     @property
     def dim(self) -> int:
-        return self.info()["dim"]
+        # Fixed for the index's lifetime; info() also sums memory_bytes() over every node, far
+        # too slow to run on each search call.
+        if self._dim is None:
+            self._dim = int(self.info()["dim"])
+        return self._dim
 
     def __len__(self) -> int:
         return self.info()["size"]

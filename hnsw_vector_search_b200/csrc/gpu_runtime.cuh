@@ -55,6 +55,10 @@ struct Workspace {
 void check(cudaError_t err, const char* what);
 void use_device(int device);
 void* device_alloc(std::size_t bytes, const char* what);
+// The device address of page-locked host memory (cudaHostAlloc / cudaMallocHost / a mapped
+// cudaHostRegister range), which kernels may read across the bus in place; nullptr for pageable
+// memory or memory the device cannot address.
+const void* mapped_host(const void* host);
 Workspace& workspace(int device);
 void reset_small(Workspace& ws);
 void raise_status(std::uint32_t code, const char* where);

@@ -168,11 +168,14 @@ float HnswIndex::dist(const float* a, const float* b) const noexcept {
 }
 
 std::size_t HnswIndex::memory_bytes() const noexcept {
-    std::size_t bytes = vectors_.data().size_bytes() + levels_.size() + layer0_.size() * sizeof(Id);
-    for (const auto& blocks : upper_) {
-        bytes += sizeof(std::vector<Id>) + blocks.size() * sizeof(Id);
+    // Every node's upper vector holds exactly level x (1 + M) ids (store() and load() size them
+    // so), which lets the levels give the total without visiting n separate allocations.
+    std::size_t blocks = 0;
+    for (const std::uint8_t level : levels_) {
+        blocks += level;
     }
-    return bytes;
+    return vectors_.data().size_bytes() + levels_.size() + layer0_.size() * sizeof(Id) +
+           upper_.size() * sizeof(std::vector<Id>) + blocks * (1 + max_links(1)) * sizeof(Id);
 }
 
 void HnswIndex::invalidate_device() noexcept {

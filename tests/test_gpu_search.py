@@ -181,6 +181,29 @@ def test_bad_queries_raise_the_reference_errors(gpu):
     assert list(c) == [5] * 4
 
 
+def test_page_locked_queries_are_read_in_place_with_the_same_results(gpu, orc, small_l2):
+    """Queries in page-locked host memory are read by the kernel across the bus instead of being
+    copied first: same bits as pageable queries and as the reference, same error reports."""
+    import torch
+    path, _, queries = small_l2
+    ix = gpu.HnswIndex.load(path)
+    ref = orc.RefHnsw.load(path)
+    pinned = torch.from_numpy(queries).pin_memory()
+    for precision in ("fp32", "bf16"):
+        o = {} if precision == "fp32" else {"precision": "bf16", "rerank": 40}
+        assert_same(ix.search_batch(pinned.numpy(), 10, 36, **o), ix.search_batch(queries.copy(), 10, 36, **o),
+                    precision)
+    assert_same(ix.search_batch(pinned.numpy()[17:530], 10, 64), ref.search_batch(queries[17:530], 10, 64, 1),
+                "pinned slice vs reference")
+    pinned[37, 2] = float("nan")
+    with pytest.raises(ValueError, match="query must not contain NaN or inf"):
+        ix.search_batch(pinned.numpy(), 10, 36)
+    cos = gpu.HnswIndex(2, "cosine", M=4, ef_construction=8)
+    cos.add(uniform_matrix(20, 2, 1))
+    with pytest.raises(ValueError, match="can't normalize a zero query"):
+        cos.search_batch(torch.zeros((3, 2)).pin_memory().numpy(), 2, 5)
+
+
 def test_bf16_traversal_is_exact_on_integer_data(gpu, small_l2):
     """Integers up to 256 are exact in bfloat16, so the BF16 traversal scores exactly what FP32
     scores and the results are the FP32 (reference) results."""

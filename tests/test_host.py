@@ -89,6 +89,9 @@ def test_serial_build_matches_reference_on_real_valued_data(vdx, orc, tmp_path, 
     mine.add(base, num_threads=1)
     mine.save(tmp_path / "mine.vdx")
     assert (tmp_path / "mine.vdx").read_bytes() == (tmp_path / "ref.vdx").read_bytes()
+    # memory_bytes (src/hnsw.cpp:207-214 of the reference) on the built and on a loaded graph.
+    assert mine.info()["memory_bytes"] == ref.info()["memory_bytes"]
+    assert vdx.HnswIndex.load(tmp_path / "ref.vdx").info()["memory_bytes"] == ref.info()["memory_bytes"]
 
 
 def test_files_round_trip_both_ways(vdx, orc, tmp_path):
