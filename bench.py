@@ -394,18 +394,26 @@ def main():
     peak, peak_kind = peaks()
     traffic = ncu_traffic(f"search_{best}")
 
-    # End to end through the public host API: pinned host queries in, results out, per step.
+    # End to end through the public host API: page-locked host queries in, results out into
+    # page-locked host arrays, per step (the kernel reads the queries and writes the results
+    # across the bus in place; every byte still moves each step).
     h_q = torch.from_numpy(queries).pin_memory().numpy()
     ef_best = r["ef"]
     opts = dict(modes)[best]
-    ix.search_batch(h_q, K, ef_best, device=local, **opts)
+    h_out = (torch.empty((nq, K), dtype=torch.int32).pin_memory().numpy().view(np.uint32),
+             torch.empty((nq, K), dtype=torch.float32).pin_memory().numpy(),
+             torch.empty(nq, dtype=torch.int32).pin_memory().numpy().view(np.uint32))
+    want = ix.search_batch(h_q, K, ef_best, device=local, **opts)
     if pg is not None:
         pg.barrier()
     e2e_total = 0.0
     for _ in range(args.steps):
+        h_out[0].fill(0)
         t0 = time.perf_counter()
-        ix.search_batch(h_q, K, ef_best, device=local, **opts)
+        ix.search_batch(h_q, K, ef_best, device=local, out=h_out, **opts)
         e2e_total += time.perf_counter() - t0
+        if not np.array_equal(h_out[0], want[0]):
+            raise RuntimeError("end-to-end results differ from the reference call's")
     if pg is not None:
         t = torch.tensor([e2e_total], device=dev)
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
@@ -442,7 +450,8 @@ def main():
             "cpu_baseline": cpu,
             "e2e": {"value": nq * world * args.steps / e2e_total, "unit": "queries/s",
                     "h2d_bytes_per_step": int(queries.nbytes),
-                    "d2h_bytes_per_step": int(nq * K * 8 + nq * 4)},
+                    "d2h_bytes_per_step": int(nq * K * 8 + nq * 4),
+                    "api": "HnswIndex.search_batch(page-locked queries, out=page-locked arrays)"},
             "gpu_launches": args.steps,
             "clocks": clock_summary,
             "bruteforce": brute,

@@ -240,16 +240,27 @@ class HnswIndex:
     def upload(self, device: int = 0, precision: str = "fp32") -> None:
         _raise(lib().vdx_index_upload(self._h, device, PRECISIONS[precision]))
 
-    def search_batch(self, queries, k: int, ef: int, **options):
+    def search_batch(self, queries, k: int, ef: int, *, out=None, **options):
         """(ids uint32 [nq, k], distances float32 [nq, k], counts uint32 [nq]); rows shorter
-        than k are padded with 0xFFFFFFFF / +inf."""
+        than k are padded with 0xFFFFFFFF / +inf. `out` = (ids, distances, counts) arrays of
+        those dtypes and shapes, C-contiguous, to fill instead of new ones; page-locked ones
+        (e.g. from torch's pin_memory) are written by the GPU in place."""
         q = _rows(queries, self.dim)
         nq = q.shape[0]
         dim = q.shape[1] if q.ndim == 2 else self.dim
         kk = max(int(k), 0)
-        ids = np.empty((nq, kk), np.uint32)
-        dists = np.empty((nq, kk), np.float32)
-        counts = np.empty(nq, np.uint32)
+        if out is None:
+            ids = np.empty((nq, kk), np.uint32)
+            dists = np.empty((nq, kk), np.float32)
+            counts = np.empty(nq, np.uint32)
+        else:
+            ids, dists, counts = out
+            for a, dt, shape, name in ((ids, np.uint32, (nq, kk), "ids"), (dists, np.float32, (nq, kk), "distances"),
+                                       (counts, np.uint32, (nq,), "counts")):
+                if not isinstance(a, np.ndarray) or a.dtype != dt or a.shape != shape or not a.flags.c_contiguous \
+                        or not a.flags.writeable:
+                    raise ValueError(f"search_batch: out {name} must be a writable C-contiguous "
+                                     f"{np.dtype(dt).name} array of shape {shape}")
         if k < 0 or ef < 0:
             raise ValueError("HnswIndex::search_batch: k and ef must be non-negative")
         opts = _options(**options)

@@ -507,9 +507,14 @@ void HnswIndex::search_batch_into(MatrixView<float> queries, std::size_t k, std:
     a.k = static_cast<std::uint32_t>(k);
     a.ef = static_cast<std::uint32_t>(ef);
     a.out_stride = static_cast<std::uint32_t>(k);
-    a.out_ids = ws.ids;
-    a.out_dists = ws.dists;
-    a.out_counts = ws.counts;
+    // Page-locked result buffers are written by the kernel in place (it only stores to them),
+    // so the results cross the bus as they are found; pageable ones are copied back after.
+    auto* ids_in_place = static_cast<std::uint32_t*>(const_cast<void*>(gpu::mapped_host(ids)));
+    auto* dists_in_place = static_cast<float*>(const_cast<void*>(gpu::mapped_host(distances)));
+    auto* counts_in_place = static_cast<std::uint32_t*>(const_cast<void*>(gpu::mapped_host(counts)));
+    a.out_ids = ids_in_place != nullptr ? ids_in_place : ws.ids;
+    a.out_dists = dists_in_place != nullptr ? dists_in_place : ws.dists;
+    a.out_counts = counts_in_place != nullptr ? counts_in_place : ws.counts;
     a.status = ws.small;
     a.claim = ws.small + 2;
     a.stats = reinterpret_cast<unsigned long long*>(ws.small + 16);
@@ -530,10 +535,17 @@ void HnswIndex::search_batch_into(MatrixView<float> queries, std::size_t k, std:
     gpu::check(dev::launch_search(a, plan, ws.stream), "search kernel");
     gpu::check(cudaMemcpyAsync(ws.small_host, ws.small, 256, cudaMemcpyDeviceToHost, ws.stream),
                "copy status");
-    gpu::check(cudaMemcpyAsync(ids, ws.ids, nq * k * 4, cudaMemcpyDeviceToHost, ws.stream), "copy ids");
-    gpu::check(cudaMemcpyAsync(distances, ws.dists, nq * k * 4, cudaMemcpyDeviceToHost, ws.stream),
-               "copy distances");
-    gpu::check(cudaMemcpyAsync(counts, ws.counts, nq * 4, cudaMemcpyDeviceToHost, ws.stream), "copy counts");
+    if (ids_in_place == nullptr) {
+        gpu::check(cudaMemcpyAsync(ids, ws.ids, nq * k * 4, cudaMemcpyDeviceToHost, ws.stream), "copy ids");
+    }
+    if (dists_in_place == nullptr) {
+        gpu::check(cudaMemcpyAsync(distances, ws.dists, nq * k * 4, cudaMemcpyDeviceToHost, ws.stream),
+                   "copy distances");
+    }
+    if (counts_in_place == nullptr) {
+        gpu::check(cudaMemcpyAsync(counts, ws.counts, nq * 4, cudaMemcpyDeviceToHost, ws.stream),
+                   "copy counts");
+    }
     gpu::check(cudaStreamSynchronize(ws.stream), "search");
     std::memcpy(ws.last_stats, ws.small_host + 16, sizeof ws.last_stats);
     gpu::raise_status(ws.small_host[0], where);

@@ -195,6 +195,18 @@ def test_page_locked_queries_are_read_in_place_with_the_same_results(gpu, orc, s
                     precision)
     assert_same(ix.search_batch(pinned.numpy()[17:530], 10, 64), ref.search_batch(queries[17:530], 10, 64, 1),
                 "pinned slice vs reference")
+    # Results written in place into page-locked buffers, and into pageable ones passed as out=.
+    nq = len(queries)
+    for make in (lambda t: t.pin_memory().numpy(), lambda t: t.numpy()):
+        out = (make(torch.full((nq, 10), 7, dtype=torch.int32)).view(np.uint32),
+               make(torch.full((nq, 10), 7.0)), make(torch.full((nq,), 7, dtype=torch.int32)).view(np.uint32))
+        got = ix.search_batch(pinned.numpy(), 10, 36, out=out)
+        assert all(g is o for g, o in zip(got, out))
+        assert_same(out, ref.search_batch(queries, 10, 36, 1), "out=")
+    with pytest.raises(ValueError, match="out distances must be"):
+        ix.search_batch(queries, 10, 36, out=(out[0], np.empty((nq, 10), np.float64), out[2]))
+    with pytest.raises(ValueError, match="out ids must be"):
+        ix.search_batch(queries, 10, 36, out=(out[0][:, :5], out[1], out[2]))
     pinned[37, 2] = float("nan")
     with pytest.raises(ValueError, match="query must not contain NaN or inf"):
         ix.search_batch(pinned.numpy(), 10, 36)
