@@ -84,4 +84,135 @@ __device__ __forceinline__ int first_unexpanded(const std::uint32_t* rid, int fr
     return r;
 }
 
+// R held in registers, for result capacities up to 64: lane l holds entries l and 32 + l
+// (distance, id with the expanded bit); entries at r and beyond hold (+inf, kNoId). The
+// shared-memory arrays (rd, rid) stay an exact mirror of R[0, r) — every write goes to both —
+// so code after the walk reads R there; the walk itself reads the registers.
+constexpr std::uint32_t kRegBeamCap = 64;
+
+struct RegBeam {
+    float d0, d1;
+    std::uint32_t i0, i1;
+};
+
+__device__ __forceinline__ void reg_beam_init(RegBeam& b, float d, std::uint32_t id, int lane) {
+    b.d0 = lane == 0 ? d : INFINITY;
+    b.i0 = lane == 0 ? id : kNoId;
+    b.d1 = INFINITY;
+    b.i1 = kNoId;
+}
+
+// R[p] for a warp-uniform p.
+__device__ __forceinline__ float reg_d(const RegBeam& b, int p) {
+    return __shfl_sync(kFull, p < 32 ? b.d0 : b.d1, p & 31);
+}
+__device__ __forceinline__ std::uint32_t reg_id(const RegBeam& b, int p) {
+    return __shfl_sync(kFull, p < 32 ? b.i0 : b.i1, p & 31);
+}
+
+__device__ __forceinline__ void reg_mark_expanded(RegBeam& b, int p, int lane) {
+    if (lane == (p & 31)) {
+        if (p < 32) {
+            b.i0 |= kExpanded;
+        } else {
+            b.i1 |= kExpanded;
+        }
+    }
+}
+
+// first_unexpanded over the registers.
+__device__ __forceinline__ int reg_first_unexpanded(const RegBeam& b, int from, int r, int lane) {
+    const std::uint32_t m0 = __ballot_sync(kFull, lane >= from && lane < r && (b.i0 & kExpanded) == 0);
+    if (m0 != 0) {
+        return __ffs(m0) - 1;
+    }
+    const int l1 = 32 + lane;
+    const std::uint32_t m1 = __ballot_sync(kFull, l1 >= from && l1 < r && (b.i1 & kExpanded) == 0);
+    return m1 != 0 ? 32 + __ffs(m1) - 1 : r;
+}
+
+// merge_round (common.cuh) over the registers, with the same steps and so the same result: the
+// full-list admission test, each candidate's position `lo` by the same binary search (probes
+// read by shuffles), the duplicate test at `lo`, the rank among admitted candidates, entries at
+// index i moved up by the number of admitted positions <= i, and everything at ef or beyond
+// dropped. The new R is scattered into the shared-memory mirror (rd, rid) and read back into
+// the registers. Returns the lowest position a candidate was kept at (0x7FFFFFFF if none).
+__device__ __forceinline__ int reg_merge_round(RegBeam& b, float* rd, std::uint32_t* rid, int& r,
+                                               int ef, float my_d, std::uint32_t my_id, bool valid,
+                                               int lane, unsigned long long& dups) {
+    if (r >= ef) {
+        const float wd = reg_d(b, r - 1);
+        const std::uint32_t wi = reg_id(b, r - 1) & kIdMask;
+        valid = valid && closer(my_d, my_id, wd, wi);
+    }
+    int lo = 0;
+    int hi = valid ? r : 0;
+    while (__any_sync(kFull, lo < hi)) {
+        const int mid = (lo + hi) >> 1;
+        const int src = mid & 31;
+        const float m0 = __shfl_sync(kFull, b.d0, src);
+        const float m1 = __shfl_sync(kFull, b.d1, src);
+        const std::uint32_t j0 = __shfl_sync(kFull, b.i0, src);
+        const std::uint32_t j1 = __shfl_sync(kFull, b.i1, src);
+        if (lo < hi) {
+            const float dm = mid < 32 ? m0 : m1;
+            const std::uint32_t im = (mid < 32 ? j0 : j1) & kIdMask;
+            if (dm < my_d || (dm == my_d && im < my_id)) {
+                lo = mid + 1;
+            } else {
+                hi = mid;
+            }
+        }
+    }
+    const std::uint32_t a0 = __shfl_sync(kFull, b.i0, lo & 31);
+    const std::uint32_t a1 = __shfl_sync(kFull, b.i1, lo & 31);
+    const bool adm = valid && !(lo < r && ((lo < 32 ? a0 : a1) & kIdMask) == my_id);
+    const std::uint32_t dupmask = __ballot_sync(kFull, valid && !adm);
+    if (lane == 0) {
+        dups += __popc(dupmask);
+    }
+    const std::uint32_t am = __ballot_sync(kFull, adm);
+    if (am == 0) {
+        return 0x7FFFFFFF;
+    }
+    int rank = 0;
+    int s0 = 0;
+    int s1 = 0;
+    for (std::uint32_t m = am; m != 0; m &= m - 1) {
+        const int j = __ffs(m) - 1;
+        const float dj = __shfl_sync(kFull, my_d, j);
+        const std::uint32_t ij = __shfl_sync(kFull, my_id, j);
+        const int lj = __shfl_sync(kFull, lo, j);
+        rank += (adm && closer(dj, ij, my_d, my_id)) ? 1 : 0;
+        s0 += lj <= lane ? 1 : 0;
+        s1 += lj <= 32 + lane ? 1 : 0;
+    }
+    const int p0 = lane + s0;
+    const int p1 = 32 + lane + s1;
+    const int newpos = lo + rank;
+    const bool keep = adm && newpos < ef;
+    if (lane < r && p0 < ef) {
+        rd[p0] = b.d0;
+        rid[p0] = b.i0;
+    }
+    if (32 + lane < r && p1 < ef) {
+        rd[p1] = b.d1;
+        rid[p1] = b.i1;
+    }
+    if (keep) {
+        rd[newpos] = my_d;
+        rid[newpos] = my_id;
+    }
+    r = min(ef, r + __popc(am));
+    __syncwarp();
+    b.d0 = lane < r ? rd[lane] : INFINITY;
+    b.i0 = lane < r ? rid[lane] : kNoId;
+    b.d1 = 32 + lane < r ? rd[32 + lane] : INFINITY;
+    b.i1 = 32 + lane < r ? rid[32 + lane] : kNoId;
+    const int low = static_cast<int>(
+        __reduce_min_sync(kFull, keep ? static_cast<std::uint32_t>(newpos) : 0x7FFFFFFFu));
+    __syncwarp();
+    return low;
+}
+
 }  // namespace vdx::dev

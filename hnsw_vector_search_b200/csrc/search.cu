@@ -180,7 +180,8 @@ __device__ __forceinline__ float stop_probability(const StopNetView& net, const 
     return 1.0F / (1.0F + __expf(-logit));
 }
 
-template <int P, bool kL2>
+// kRegR: R in registers (RegBeam, result capacity up to 64) instead of shared memory.
+template <int P, bool kL2, bool kRegR>
 __global__ void __launch_bounds__(256) search_kernel(const SearchArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = static_cast<int>(threadIdx.x & 31);
@@ -409,6 +410,10 @@ __global__ void __launch_bounds__(256) search_kernel(const SearchArgs a) {
             rid[0] = cur;
         }
         __syncwarp();
+        RegBeam rb{};
+        if constexpr (kRegR) {
+            reg_beam_init(rb, curd, cur, lane);
+        }
         int r = 1;
         int scan = 0;
         int slot = 0;
@@ -416,11 +421,22 @@ __global__ void __launch_bounds__(256) search_kernel(const SearchArgs a) {
         const float d_entry = curd;
         int hops = 0;
         for (std::uint32_t step = 0; step <= g.n; ++step) {
-            const int p = first_unexpanded(rid, scan, r, lane);
-            if (p >= r) {
-                break;
+            int p;
+            std::uint32_t node;
+            if constexpr (kRegR) {
+                p = reg_first_unexpanded(rb, scan, r, lane);
+                if (p >= r) {
+                    break;
+                }
+                node = reg_id(rb, p) & kIdMask;
+                reg_mark_expanded(rb, p, lane);
+            } else {
+                p = first_unexpanded(rid, scan, r, lane);
+                if (p >= r) {
+                    break;
+                }
+                node = rid[p] & kIdMask;
             }
-            const std::uint32_t node = rid[p] & kIdMask;
             __syncwarp();
             if (lane == 0) {
                 rid[p] = node | kExpanded;
@@ -498,26 +514,52 @@ __global__ void __launch_bounds__(256) search_kernel(const SearchArgs a) {
                     float bd;
                     std::uint32_t bi;
                     warp_argmin(my_d, my_id, bd, bi);
-                    const bool admissible =
-                        bi != kNoId && (r < ef || closer(bd, bi, rd[r - 1], rid[r - 1] & kIdMask));
-                    const int pu = first_unexpanded(rid, scan, r, lane);
-                    std::uint32_t nxt = admissible ? bi : kNoId;
-                    if (pu < r) {
-                        const std::uint32_t ui = rid[pu] & kIdMask;
-                        if (!admissible || closer(rd[pu], ui, bd, bi)) {
+                    std::uint32_t nxt;
+                    if constexpr (kRegR) {
+                        const float wd = reg_d(rb, r - 1);
+                        const std::uint32_t wi = reg_id(rb, r - 1) & kIdMask;
+                        const bool admissible = bi != kNoId && (r < ef || closer(bd, bi, wd, wi));
+                        const int pu = reg_first_unexpanded(rb, scan, r, lane);
+                        nxt = admissible ? bi : kNoId;
+                        const int pq = pu < r ? pu : 0;
+                        const float ud = reg_d(rb, pq);
+                        const std::uint32_t ui = reg_id(rb, pq) & kIdMask;
+                        if (pu < r && (!admissible || closer(ud, ui, bd, bi))) {
                             nxt = ui;
+                        }
+                    } else {
+                        const bool admissible =
+                            bi != kNoId && (r < ef || closer(bd, bi, rd[r - 1], rid[r - 1] & kIdMask));
+                        const int pu = first_unexpanded(rid, scan, r, lane);
+                        nxt = admissible ? bi : kNoId;
+                        if (pu < r) {
+                            const std::uint32_t ui = rid[pu] & kIdMask;
+                            if (!admissible || closer(rd[pu], ui, bd, bi)) {
+                                nxt = ui;
+                            }
                         }
                     }
                     __syncwarp();
                     prefetch_links(nxt);
                 }
-                const int low = merge_round(rd, rid, r, ef, my_d, my_id, valid, ap, lane, c_dup);
+                int low;
+                if constexpr (kRegR) {
+                    low = reg_merge_round(rb, rd, rid, r, ef, my_d, my_id, valid, lane, c_dup);
+                } else {
+                    low = merge_round(rd, rid, r, ef, my_d, my_id, valid, ap, lane, c_dup);
+                }
                 scan = min(scan, low);
             }
             if (f == 0) {
                 // Nothing scored: the next expansion is R's first unexpanded entry.
-                const int pu = first_unexpanded(rid, scan, r, lane);
-                prefetch_links(pu < r ? rid[pu] & kIdMask : kNoId);
+                if constexpr (kRegR) {
+                    const int pu = reg_first_unexpanded(rb, scan, r, lane);
+                    const std::uint32_t ui = reg_id(rb, pu < r ? pu : 0) & kIdMask;
+                    prefetch_links(pu < r ? ui : kNoId);
+                } else {
+                    const int pu = first_unexpanded(rid, scan, r, lane);
+                    prefetch_links(pu < r ? rid[pu] & kIdMask : kNoId);
+                }
             }
             slot ^= 1;
             ++hops;
@@ -647,10 +689,10 @@ __global__ void __launch_bounds__(256) search_kernel(const SearchArgs a) {
 
 std::uint32_t round_up(std::uint32_t x, std::uint32_t m) { return (x + m - 1) / m * m; }
 
-template <int P, bool kL2>
+template <int P, bool kL2, bool kRegR>
 cudaError_t launch_typed(SearchArgs& args, const SearchPlan& plan, std::size_t smem,
                          cudaStream_t stream) {
-    auto* kernel = &search_kernel<P, kL2>;
+    auto* kernel = &search_kernel<P, kL2, kRegR>;
     cudaError_t err =
         cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (err != cudaSuccess) {
@@ -771,21 +813,30 @@ std::uint32_t search_warps(SearchArgs& args, const SearchPlan& plan) {
         return per_sm > 0 ? per_sm : 1;
     };
     const bool l2 = args.g.metric == 0;
-    int per_sm = 1;
+    // The kernel launch_search will pick (the register-beam variants for small capacities).
+    const bool reg = plan.efcap <= kRegBeamCap;
+    const void* kernel = nullptr;
     switch (args.g.precision) {
         case 0:
-            per_sm = l2 ? per_sm_of(reinterpret_cast<const void*>(&search_kernel<kFP32, true>))
-                        : per_sm_of(reinterpret_cast<const void*>(&search_kernel<kFP32, false>));
+            kernel = reg ? (l2 ? reinterpret_cast<const void*>(&search_kernel<kFP32, true, true>)
+                               : reinterpret_cast<const void*>(&search_kernel<kFP32, false, true>))
+                         : (l2 ? reinterpret_cast<const void*>(&search_kernel<kFP32, true, false>)
+                               : reinterpret_cast<const void*>(&search_kernel<kFP32, false, false>));
             break;
         case 1:
-            per_sm = l2 ? per_sm_of(reinterpret_cast<const void*>(&search_kernel<kBF16, true>))
-                        : per_sm_of(reinterpret_cast<const void*>(&search_kernel<kBF16, false>));
+            kernel = reg ? (l2 ? reinterpret_cast<const void*>(&search_kernel<kBF16, true, true>)
+                               : reinterpret_cast<const void*>(&search_kernel<kBF16, false, true>))
+                         : (l2 ? reinterpret_cast<const void*>(&search_kernel<kBF16, true, false>)
+                               : reinterpret_cast<const void*>(&search_kernel<kBF16, false, false>));
             break;
         default:
-            per_sm = l2 ? per_sm_of(reinterpret_cast<const void*>(&search_kernel<kFP8, true>))
-                        : per_sm_of(reinterpret_cast<const void*>(&search_kernel<kFP8, false>));
+            kernel = reg ? (l2 ? reinterpret_cast<const void*>(&search_kernel<kFP8, true, true>)
+                               : reinterpret_cast<const void*>(&search_kernel<kFP8, false, true>))
+                         : (l2 ? reinterpret_cast<const void*>(&search_kernel<kFP8, true, false>)
+                               : reinterpret_cast<const void*>(&search_kernel<kFP8, false, false>));
             break;
     }
+    const int per_sm = per_sm_of(kernel);
     return static_cast<std::uint32_t>(sms * per_sm * plan.warps_per_block);
 }
 
@@ -813,16 +864,29 @@ void bind_global_visited(SearchArgs& args, const SearchPlan& plan, void* buffer,
 cudaError_t launch_search(SearchArgs& args, const SearchPlan& plan, cudaStream_t stream) {
     const std::size_t smem = plan_search(args, plan);
     const bool l2 = args.g.metric == 0;
+    if (plan.efcap <= kRegBeamCap) {
+        switch (args.g.precision) {
+            case 0:
+                return l2 ? launch_typed<kFP32, true, true>(args, plan, smem, stream)
+                          : launch_typed<kFP32, false, true>(args, plan, smem, stream);
+            case 1:
+                return l2 ? launch_typed<kBF16, true, true>(args, plan, smem, stream)
+                          : launch_typed<kBF16, false, true>(args, plan, smem, stream);
+            default:
+                return l2 ? launch_typed<kFP8, true, true>(args, plan, smem, stream)
+                          : launch_typed<kFP8, false, true>(args, plan, smem, stream);
+        }
+    }
     switch (args.g.precision) {
         case 0:
-            return l2 ? launch_typed<kFP32, true>(args, plan, smem, stream)
-                      : launch_typed<kFP32, false>(args, plan, smem, stream);
+            return l2 ? launch_typed<kFP32, true, false>(args, plan, smem, stream)
+                      : launch_typed<kFP32, false, false>(args, plan, smem, stream);
         case 1:
-            return l2 ? launch_typed<kBF16, true>(args, plan, smem, stream)
-                      : launch_typed<kBF16, false>(args, plan, smem, stream);
+            return l2 ? launch_typed<kBF16, true, false>(args, plan, smem, stream)
+                      : launch_typed<kBF16, false, false>(args, plan, smem, stream);
         default:
-            return l2 ? launch_typed<kFP8, true>(args, plan, smem, stream)
-                      : launch_typed<kFP8, false>(args, plan, smem, stream);
+            return l2 ? launch_typed<kFP8, true, false>(args, plan, smem, stream)
+                      : launch_typed<kFP8, false, false>(args, plan, smem, stream);
     }
 }
 
