@@ -425,6 +425,7 @@ def main():
     if pg is not None:
         pg.barrier()
     if rank == 0:
+        kernels_per_step = int(v.lib().vdx_search_kernels_last())  # the e2e calls' launches
         line = {
             "metric": METRIC, "value": r["qps"], "unit": "queries/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
@@ -452,7 +453,7 @@ def main():
                     "h2d_bytes_per_step": int(queries.nbytes),
                     "d2h_bytes_per_step": int(nq * K * 8 + nq * 4),
                     "api": "HnswIndex.search_batch(page-locked queries, out=page-locked arrays)"},
-            "gpu_launches": args.steps,
+            "gpu_launches": args.steps * kernels_per_step,
             "clocks": clock_summary,
             "bruteforce": brute,
         }

@@ -96,6 +96,7 @@ Batcher::Batcher(const HnswIndex& idx, int dev, Precision prec, std::uint32_t ma
         c.d_dists = dalloc<float>(rows_out, "batch distances");
         c.d_counts = dalloc<std::uint32_t>(max_q, "batch counts");
         c.d_work = dalloc<std::uint32_t>(kWorkWords, "batch work words");
+        c.d_order = dalloc<std::uint32_t>(3 * static_cast<std::size_t>(max_q), "batch order");
         c.h_queries = halloc<float>(rows_q);
         c.h_k = halloc<std::uint32_t>(max_q);
         c.h_ef = halloc<std::uint32_t>(max_q);
@@ -129,7 +130,7 @@ Batcher::~Batcher() {
         for (void* p : {static_cast<void*>(c.d_queries), static_cast<void*>(c.d_k),
                         static_cast<void*>(c.d_ef), static_cast<void*>(c.d_nq),
                         static_cast<void*>(c.d_ids), static_cast<void*>(c.d_dists),
-                        static_cast<void*>(c.d_counts), static_cast<void*>(c.d_work), c.d_visited}) {
+                        static_cast<void*>(c.d_counts), static_cast<void*>(c.d_work), static_cast<void*>(c.d_order), c.d_visited}) {
             cudaFree(p);
         }
         for (void* p : {static_cast<void*>(c.h_queries), static_cast<void*>(c.h_k),
@@ -195,6 +196,9 @@ SearchArgs Batcher::args(const EfClass& c, const SearchPlan& plan) {
     a.status = c.d_work;
     a.claim = c.d_work + 2;
     a.stats = reinterpret_cast<unsigned long long*>(c.d_work + 16);
+    a.entry_ids = c.d_order;
+    a.entry_d = reinterpret_cast<float*>(c.d_order + max_queries);
+    a.order = c.d_order + 2 * static_cast<std::size_t>(max_queries);
     if (precision != Precision::FP32) {
         // As the batch search: an FP32 re-rank of the best 4 * k of each query.
         a.rerank = kRerankPerK * max_k;

@@ -34,6 +34,7 @@ struct EfClass {
                   *h_counts = nullptr, *h_work = nullptr;
     float* h_dists = nullptr;
     std::vector<std::uint32_t> rows;      // batch row of each staged position
+    std::uint32_t* d_order = nullptr;     // ordered-launch scratch: 3 words per query
     void* d_visited = nullptr;            // global visited tables (large-ef plans), grow-only
     std::uint32_t visited_stride = 0;
     std::uint32_t visited_warps = 0;

@@ -268,6 +268,8 @@ vdx_status vdx_index_upload(const vdx_index* index, int32_t device, uint32_t pre
 
 uint64_t vdx_work_words(void) { return 64; }
 
+uint32_t vdx_search_kernels_last(void) { return static_cast<uint32_t>(vdx::dev::search_kernels_per_launch()); }
+
 vdx_status vdx_search_batch_device(const vdx_index* index, const float* d_queries, uint64_t nq,
                                    uint64_t dim, const uint32_t* d_k, const uint32_t* d_ef,
                                    uint32_t k_uniform, uint32_t ef_uniform, uint32_t out_stride,
@@ -320,6 +322,10 @@ vdx_status vdx_search_batch_device(const vdx_index* index, const float* d_querie
         // Per-query ef: the capacity must cover the largest; the caller's uniform ef bounds it.
         const uint64_t cap = std::min<uint64_t>(std::max<uint64_t>(ef_uniform, kk), h.size());
         const vdx::dev::SearchPlan plan = vdx::dev::default_plan(g.view, static_cast<uint32_t>(cap));
+        const vdx::gpu::OrderScratch order(o.device, nq, s);
+        a.entry_ids = order.entry_ids();
+        a.entry_d = order.entry_d();
+        a.order = order.order();
         vdx::gpu::check(vdx::dev::launch_search(a, plan, s), "search kernel");
     });
 }

@@ -19,6 +19,7 @@
 #include <format>
 #include <limits>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -83,6 +84,44 @@ void use_device(int device) {
         throw std::invalid_argument(std::format("vdx: device {} does not exist ({} found)", device, count));
     }
     check(cudaSetDevice(device), "cudaSetDevice");
+}
+
+namespace {
+
+cudaMemPool_t order_pool(int device) {
+    static std::mutex m;
+    static std::vector<cudaMemPool_t> pools;
+    const std::scoped_lock lock(m);
+    if (pools.size() <= static_cast<std::size_t>(device)) {
+        pools.resize(device + 1, nullptr);
+    }
+    if (pools[device] == nullptr) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        cudaMemPool_t pool = nullptr;
+        check(cudaMemPoolCreate(&pool, &props), "cudaMemPoolCreate");
+        std::uint64_t keep = ~std::uint64_t{0};
+        check(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep), "cudaMemPoolSetAttribute");
+        pools[device] = pool;
+    }
+    return pools[device];
+}
+
+}  // namespace
+
+OrderScratch::OrderScratch(int device, std::size_t nq, cudaStream_t stream) : nq_(nq), stream_(stream) {
+    void* p = nullptr;
+    check(cudaMallocFromPoolAsync(&p, std::max<std::size_t>(nq, 1) * 12, order_pool(device), stream),
+          "order scratch");
+    words_ = static_cast<std::uint32_t*>(p);
+}
+
+OrderScratch::~OrderScratch() {
+    if (words_ != nullptr) {
+        cudaFreeAsync(words_, stream_);
+    }
 }
 
 const void* mapped_host(const void* host) {
@@ -532,6 +571,10 @@ void HnswIndex::search_batch_into(MatrixView<float> queries, std::size_t k, std:
         void* buf = ws.visited_for(plan.global_slots, warps);
         dev::bind_global_visited(a, plan, buf, ws.visited_stride, ws.visited_warps);
     }
+    gpu::OrderScratch order(options.device, nq, ws.stream);
+    a.entry_ids = order.entry_ids();
+    a.entry_d = order.entry_d();
+    a.order = order.order();
     gpu::check(dev::launch_search(a, plan, ws.stream), "search kernel");
     gpu::check(cudaMemcpyAsync(ws.small_host, ws.small, 256, cudaMemcpyDeviceToHost, ws.stream),
                "copy status");

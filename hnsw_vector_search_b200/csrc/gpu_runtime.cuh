@@ -52,6 +52,25 @@ struct Workspace {
     void* visited_for(std::uint32_t slots, std::uint32_t warps);
 };
 
+// Scratch of an ordered search launch (three words per query: layer-0 entry ids, entry
+// distances, claim order), allocated and freed in stream order from a per-device pool that keeps
+// its memory, so launches on different streams never share it and nothing synchronizes.
+class OrderScratch {
+public:
+    OrderScratch(int device, std::size_t nq, cudaStream_t stream);
+    ~OrderScratch();
+    OrderScratch(const OrderScratch&) = delete;
+    OrderScratch& operator=(const OrderScratch&) = delete;
+    std::uint32_t* entry_ids() const { return words_; }
+    float* entry_d() const { return reinterpret_cast<float*>(words_ + nq_); }
+    std::uint32_t* order() const { return words_ + 2 * nq_; }
+
+private:
+    std::uint32_t* words_ = nullptr;
+    std::size_t nq_ = 0;
+    cudaStream_t stream_ = nullptr;
+};
+
 void check(cudaError_t err, const char* what);
 void use_device(int device);
 void* device_alloc(std::size_t bytes, const char* what);

@@ -230,11 +230,19 @@ __global__ void __launch_bounds__(256) search_kernel(const SearchArgs a) {
     for (;;) {
         std::uint32_t qi = 0;
         if (lane == 0) {
-            qi = atomicAdd(a.claim, 1u);
+            qi = atomicAdd(a.pass == 2 ? a.claim + 1 : a.claim, 1u);
         }
         qi = __shfl_sync(kFull, qi, 0);
         if (qi >= nq) {
             break;
+        }
+        if (a.pass == 2) {
+            qi = a.order[qi];
+            if (a.entry_ids[qi] == kNoId) {
+                continue;  // failed its checks in the descent pass, which wrote its row
+            }
+        } else if (a.pass == 1 && lane == 0) {
+            a.entry_ids[qi] = kNoId;  // until the descent below completes
         }
         const std::uint32_t k = a.k_per_q != nullptr ? a.k_per_q[qi] : a.k;
         std::uint32_t efq = a.ef_per_q != nullptr ? a.ef_per_q[qi] : a.ef;
@@ -292,10 +300,12 @@ __global__ void __launch_bounds__(256) search_kernel(const SearchArgs a) {
             }
             __syncwarp();
         }
-        ++c_q;
+        if (a.pass != 2) {
+            ++c_q;
+        }
         float qlen = 0.0F;
         float proj[4] = {0.0F, 0.0F, 0.0F, 0.0F};
-        if (learned || tracing) {
+        if ((learned || tracing) && a.pass != 1) {
             qlen = sqrtf(warp_raw<kFP32, false>(q, reinterpret_cast<const unsigned char*>(q), g.dim,
                                                 g.row32 * 4, lane));
             const float inv = 1.0F / fmaxf(qlen, 1e-20F);
@@ -308,74 +318,89 @@ __global__ void __launch_bounds__(256) search_kernel(const SearchArgs a) {
         }
         std::uint32_t trace_points = 0;
 
-        // 2. Entry point and greedy descent.
+        // 2. Entry point and greedy descent (in the layer-0 pass of an ordered launch, the
+        // descent pass's result).
         std::uint32_t cur = g.entry;
-        if (lane == 0) {
-            fresh[0] = cur;
-        }
-        __syncwarp();
-        gather_rows(rows, stride_s, vecs, fresh, 1, g.row_bytes, shift, lane);
-        cp_async_wait<0>();
-        __syncwarp();
-        float curd = lane_distance<P, kL2>(q, rows, g.dim, g.row_bytes);
-        ++c_du;
-        c_rb += g.row_bytes;
-        for (int layer = static_cast<int>(g.max_level); layer >= 1; --layer) {
-            for (std::uint32_t hop = 0; hop <= g.n; ++hop) {
-                const std::uint32_t* block =
-                    g.links_up + static_cast<std::size_t>(g.upper_at[cur] + layer - 1) * g.stride_up;
-                int f = 0;
-                for (std::uint32_t c0 = 0; c0 < g.cap_up; c0 += 32) {
-                    const std::uint32_t j = c0 + lane;
-                    std::uint32_t id = j < g.cap_up ? block[j] : kNoId;
-                    if (id != kNoId && id >= g.n) {
-                        report(a.status, kErrBounds, qi);
-                        id = kNoId;
+        float curd = 0.0F;
+        if (a.pass == 2) {
+            cur = a.entry_ids[qi];
+            curd = a.entry_d[qi];
+        } else {
+            if (lane == 0) {
+                fresh[0] = cur;
+            }
+            __syncwarp();
+            gather_rows(rows, stride_s, vecs, fresh, 1, g.row_bytes, shift, lane);
+            cp_async_wait<0>();
+            __syncwarp();
+            curd = lane_distance<P, kL2>(q, rows, g.dim, g.row_bytes);
+            ++c_du;
+            c_rb += g.row_bytes;
+            for (int layer = static_cast<int>(g.max_level); layer >= 1; --layer) {
+                for (std::uint32_t hop = 0; hop <= g.n; ++hop) {
+                    const std::uint32_t* block =
+                        g.links_up + static_cast<std::size_t>(g.upper_at[cur] + layer - 1) * g.stride_up;
+                    int f = 0;
+                    for (std::uint32_t c0 = 0; c0 < g.cap_up; c0 += 32) {
+                        const std::uint32_t j = c0 + lane;
+                        std::uint32_t id = j < g.cap_up ? block[j] : kNoId;
+                        if (id != kNoId && id >= g.n) {
+                            report(a.status, kErrBounds, qi);
+                            id = kNoId;
+                        }
+                        const bool valid = id != kNoId;
+                        const std::uint32_t m = __ballot_sync(kFull, valid);
+                        if (valid) {
+                            fresh[f + __popc(m & ((1u << lane) - 1u))] = id;
+                        }
+                        f += __popc(m);
                     }
-                    const bool valid = id != kNoId;
-                    const std::uint32_t m = __ballot_sync(kFull, valid);
-                    if (valid) {
-                        fresh[f + __popc(m & ((1u << lane) - 1u))] = id;
+                    __syncwarp();
+                    c_lb += 4ull * (1 + f);
+                    float best_d = INFINITY;
+                    int best_i = 0x7FFFFFFF;
+                    for (int s0 = 0; s0 < f; s0 += rounds_cap) {
+                        const int cnt = min(rounds_cap, f - s0);
+                        gather_rows(rows, stride_s, vecs, fresh + s0, cnt, g.row_bytes, shift, lane);
+                        cp_async_wait<0>();
+                        __syncwarp();
+                        const float pd = pair_distance<P, kL2>(q, my_row, g.dim, g.row_bytes, half);
+                        float d = INFINITY;
+                        int idx = 0x7FFFFFFF;
+                        if (lane < cnt) {
+                            d = pd;
+                            idx = s0 + lane;
+                        }
+                        // The first strict minimum in link order: smallest (distance, position).
+                        {
+                            std::uint32_t bidx;
+                            warp_argmin(d, static_cast<std::uint32_t>(idx), d, bidx);
+                            idx = static_cast<int>(bidx);
+                        }
+                        if (d < best_d) {
+                            best_d = d;
+                            best_i = idx;
+                        }
+                        __syncwarp();
                     }
-                    f += __popc(m);
+                    c_du += f;
+                    c_rb += static_cast<unsigned long long>(f) * g.row_bytes;
+                    if (f > 0 && best_d < curd) {
+                        cur = fresh[best_i];
+                        curd = best_d;
+                        __syncwarp();
+                    } else {
+                        break;
+                    }
                 }
+            }
+            if (a.pass == 1) {
                 __syncwarp();
-                c_lb += 4ull * (1 + f);
-                float best_d = INFINITY;
-                int best_i = 0x7FFFFFFF;
-                for (int s0 = 0; s0 < f; s0 += rounds_cap) {
-                    const int cnt = min(rounds_cap, f - s0);
-                    gather_rows(rows, stride_s, vecs, fresh + s0, cnt, g.row_bytes, shift, lane);
-                    cp_async_wait<0>();
-                    __syncwarp();
-                    const float pd = pair_distance<P, kL2>(q, my_row, g.dim, g.row_bytes, half);
-                    float d = INFINITY;
-                    int idx = 0x7FFFFFFF;
-                    if (lane < cnt) {
-                        d = pd;
-                        idx = s0 + lane;
-                    }
-                    // The first strict minimum in link order: smallest (distance, position).
-                    {
-                        std::uint32_t bidx;
-                        warp_argmin(d, static_cast<std::uint32_t>(idx), d, bidx);
-                        idx = static_cast<int>(bidx);
-                    }
-                    if (d < best_d) {
-                        best_d = d;
-                        best_i = idx;
-                    }
-                    __syncwarp();
+                if (lane == 0) {
+                    a.entry_d[qi] = curd;
+                    a.entry_ids[qi] = cur;
                 }
-                c_du += f;
-                c_rb += static_cast<unsigned long long>(f) * g.row_bytes;
-                if (f > 0 && best_d < curd) {
-                    cur = fresh[best_i];
-                    curd = best_d;
-                    __syncwarp();
-                } else {
-                    break;
-                }
+                continue;
             }
         }
 
@@ -689,6 +714,82 @@ __global__ void __launch_bounds__(256) search_kernel(const SearchArgs a) {
 
 std::uint32_t round_up(std::uint32_t x, std::uint32_t m) { return (x + m - 1) / m * m; }
 
+// The claim order of an ordered launch's layer-0 pass: queries by their layer-0 entry distance,
+// farthest first (the cost of a query's layer-0 walk grows with it), by a counting sort on the
+// top 12 bits of the distance's order-preserving integer image (buckets a factor of ~1.09
+// wide; order within a bucket is arbitrary). Queries that failed their checks go last. One
+// block: the histogram and its scan live in shared memory.
+constexpr int kOrderBuckets = 4096;
+constexpr int kOrderThreads = 1024;
+
+__device__ __forceinline__ std::uint32_t order_bucket(const SearchArgs& a, std::uint32_t i) {
+    if (a.entry_ids[i] == kNoId) {
+        return kOrderBuckets - 1;
+    }
+    std::uint32_t u = __float_as_uint(a.entry_d[i]);
+    u = (u & 0x80000000u) != 0 ? ~u : (u | 0x80000000u);
+    const std::uint32_t b = (kOrderBuckets - 1) - (u >> 20);
+    return b < kOrderBuckets - 2 ? b : kOrderBuckets - 2;
+}
+
+__global__ void __launch_bounds__(kOrderThreads) order_kernel(const SearchArgs a) {
+    __shared__ std::uint32_t count[kOrderBuckets];
+    __shared__ std::uint32_t warp_sum[kOrderThreads / 32];
+    const std::uint32_t nq = a.nq_device != nullptr ? min(*a.nq_device, a.nq) : a.nq;
+    const int t = static_cast<int>(threadIdx.x);
+    for (int b = t; b < kOrderBuckets; b += kOrderThreads) {
+        count[b] = 0;
+    }
+    __syncthreads();
+    for (std::uint32_t i = t; i < nq; i += kOrderThreads) {
+        atomicAdd(count + order_bucket(a, i), 1u);
+    }
+    __syncthreads();
+    // Exclusive scan: each thread owns four consecutive buckets.
+    constexpr int kPer = kOrderBuckets / kOrderThreads;
+    std::uint32_t own[kPer];
+    std::uint32_t sum = 0;
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) {
+        own[j] = count[t * kPer + j];
+        sum += own[j];
+    }
+    const int lane = t & 31;
+    std::uint32_t incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const std::uint32_t v = __shfl_up_sync(kFull, incl, o);
+        incl += lane >= o ? v : 0u;
+    }
+    if (lane == 31) {
+        warp_sum[t >> 5] = incl;
+    }
+    __syncthreads();
+    if (t < 32) {
+        const std::uint32_t w = warp_sum[t];
+        std::uint32_t wi = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const std::uint32_t v = __shfl_up_sync(kFull, wi, o);
+            wi += t >= o ? v : 0u;
+        }
+        warp_sum[t] = wi - w;
+    }
+    __syncthreads();
+    std::uint32_t base = warp_sum[t >> 5] + incl - sum;
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) {
+        count[t * kPer + j] = base;
+        base += own[j];
+    }
+    __syncthreads();
+    for (std::uint32_t i = t; i < nq; i += kOrderThreads) {
+        a.order[atomicAdd(count + order_bucket(a, i), 1u)] = i;
+    }
+}
+
+thread_local int g_last_kernels = 1;
+
 template <int P, bool kL2, bool kRegR>
 cudaError_t launch_typed(SearchArgs& args, const SearchPlan& plan, std::size_t smem,
                          cudaStream_t stream) {
@@ -727,7 +828,24 @@ cudaError_t launch_typed(SearchArgs& args, const SearchPlan& plan, std::size_t s
     } else {
         args.gvisited = nullptr;
     }
+    if (args.entry_ids == nullptr || args.entry_d == nullptr || args.order == nullptr) {
+        args.pass = 0;
+        kernel<<<blocks, threads, smem, stream>>>(args);
+        g_last_kernels = 1;
+        return cudaGetLastError();
+    }
+    args.pass = 1;
     kernel<<<blocks, threads, smem, stream>>>(args);
+    if (err = cudaGetLastError(); err != cudaSuccess) {
+        return err;
+    }
+    order_kernel<<<1, kOrderThreads, 0, stream>>>(args);
+    if (err = cudaGetLastError(); err != cudaSuccess) {
+        return err;
+    }
+    args.pass = 2;
+    kernel<<<blocks, threads, smem, stream>>>(args);
+    g_last_kernels = 3;
     return cudaGetLastError();
 }
 
@@ -890,6 +1008,6 @@ cudaError_t launch_search(SearchArgs& args, const SearchPlan& plan, cudaStream_t
     }
 }
 
-int search_kernels_per_launch() { return 1; }
+int search_kernels_per_launch() { return g_last_kernels; }
 
 }  // namespace vdx::dev

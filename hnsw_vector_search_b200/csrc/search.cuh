@@ -91,6 +91,15 @@ struct SearchArgs {
     float stop_threshold = 0.5F;
     std::uint32_t stop_min_hops = 16;
     TraceArgs trace{};
+    // Ordered launch (all three non-null, nq words each): a descent pass writes each query's
+    // layer-0 entry (id, distance; id 0xFFFFFFFF for a query that failed its checks), the queries
+    // are ordered by that distance, farthest first, and the layer-0 pass claims them in that
+    // order, so the queries that will take longest start first and the grid's tail is short.
+    std::uint32_t* entry_ids = nullptr;
+    float* entry_d = nullptr;
+    std::uint32_t* order = nullptr;
+    std::uint32_t pass = 0;                // set by launch_search: 0 whole search, 1 descent,
+                                           // 2 layer 0 from the entries, in `order`
     // Per-warp shared-memory layout (bytes), filled by plan_search().
     std::uint32_t efcap = 0, hash_slots = 0, rows_cap = 0, warp_bytes = 0;
     std::uint32_t off_r = 0, off_hash = 0, off_links = 0, off_rows = 0, off_fresh = 0, off_ap = 0;
@@ -126,11 +135,13 @@ std::size_t global_visited_bytes(std::uint32_t stride, std::uint32_t warps);
 void bind_global_visited(SearchArgs& args, const SearchPlan& plan, void* buffer,
                          std::uint32_t stride, std::uint32_t warps);
 
-// Launches the search for args.nq queries on `stream` (status, claim and stats must be zeroed
-// on that stream first). Returns the CUDA error of the launch.
+// Launches the search for args.nq queries on `stream` (status, claim, claim + 1 and stats must
+// be zeroed on that stream first): one kernel, or with entry_ids / entry_d / order set the
+// ordered three (descent pass, order_kernel, layer-0 pass). Returns the CUDA error of the
+// launches.
 cudaError_t launch_search(SearchArgs& args, const SearchPlan& plan, cudaStream_t stream);
 
-// Kernels launched by the last launch_search (for launch accounting).
+// Kernels launched by this thread's last launch_search (for launch accounting).
 int search_kernels_per_launch();
 
 }  // namespace vdx::dev

@@ -142,8 +142,15 @@ VDX_API vdx_status vdx_index_upload(const vdx_index* index, int32_t device, uint
  * k_uniform / ef_uniform; result rows are out_stride wide. d_work is caller-owned device memory
  * of vdx_work_words() u32 words: [0] error code (0 = ok; 1 non-finite query, 2 zero cosine
  * query, 3 corrupt device graph, 4 ef above capacity), [1] the lowest failing row, [16..] the
- * 64-bit statistics words. The call does not wait for the kernel. */
+ * 64-bit statistics words. The call does not wait for the kernel. The search runs as three
+ * kernels (an upper-layer descent for every query, a one-block ordering of the queries by their
+ * layer-0 entry distance, the layer-0 searches, farthest entries first so the costliest start
+ * first), with 12 bytes per query of scratch taken from and returned to a library-owned
+ * stream-ordered pool on `stream`. */
 VDX_API uint64_t vdx_work_words(void);
+/* Kernels the calling thread's last HNSW search launched (3 for the ordered search above and
+ * vdx_search_batch, 1 for vdx_search_batch_device_noalloc), for launch accounting. */
+VDX_API uint32_t vdx_search_kernels_last(void);
 VDX_API vdx_status vdx_search_batch_device(const vdx_index* index, const float* d_queries,
                                            uint64_t nq, uint64_t dim, const uint32_t* d_k,
                                            const uint32_t* d_ef, uint32_t k_uniform,
