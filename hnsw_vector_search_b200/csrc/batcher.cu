@@ -388,6 +388,9 @@ std::vector<TunedPlan> Batcher::autotune(const float* queries, std::uint32_t nq,
         for (const SearchPlan& base : bases) {
             const bool global = base.global_slots > 0;
             for (const int warps : {2, 4, 8}) {
+                if (warps > max_warps_per_block(graph_view, base.efcap)) {
+                    continue;
+                }
                 for (const std::uint32_t rows : {8u, 16u, 32u}) {
                     // Visited-filter size: shared-memory slots, or global slots for large ef.
                     const std::uint32_t mid = global ? base.global_slots : base.hash_slots;

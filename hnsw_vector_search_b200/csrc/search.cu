@@ -180,9 +180,20 @@ __device__ __forceinline__ float stop_probability(const StopNetView& net, const 
     return 1.0F / (1.0F + __expf(-logit));
 }
 
+// Launch bounds. The register-beam kernels over BF16 / FP8 rows need ~10 KB of shared memory
+// per warp, room for 20 resident warps per SM, but at the 128 registers the compiler picks under
+// 256 threads only 16 fit: they are held to 96 registers (blocks of at most 4 warps, 5 per SM;
+// 5-6 % faster at ef 36-64 on the 1M x 128 workload, results identical). The others are bound
+// by shared memory before registers and keep the compiler's choice (minimum blocks 0: none).
+template <int P, bool kRegR>
+constexpr bool kLowRegs = kRegR && P != kFP32;
+template <int P, bool kRegR>
+constexpr int kMaxThreads = kLowRegs<P, kRegR> ? 128 : 256;
+
 // kRegR: R in registers (RegBeam, result capacity up to 64) instead of shared memory.
 template <int P, bool kL2, bool kRegR>
-__global__ void __launch_bounds__(256) search_kernel(const SearchArgs a) {
+__global__ void __launch_bounds__(kMaxThreads<P, kRegR>, kLowRegs<P, kRegR> ? 5 : 0)
+    search_kernel(const SearchArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = static_cast<int>(threadIdx.x & 31);
     const int warp = static_cast<int>(threadIdx.x >> 5);
@@ -794,6 +805,9 @@ template <int P, bool kL2, bool kRegR>
 cudaError_t launch_typed(SearchArgs& args, const SearchPlan& plan, std::size_t smem,
                          cudaStream_t stream) {
     auto* kernel = &search_kernel<P, kL2, kRegR>;
+    if (plan.warps_per_block < 1 || plan.warps_per_block * 32 > kMaxThreads<P, kRegR>) {
+        return cudaErrorInvalidValue;  // a plan beyond max_warps_per_block
+    }
     cudaError_t err =
         cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (err != cudaSuccess) {
@@ -877,6 +891,11 @@ std::size_t plan_search(SearchArgs& a, const SearchPlan& plan) {
     off += (kHist + kHidden) * 4;
     a.warp_bytes = round_up(off, 16);
     return static_cast<std::size_t>(a.warp_bytes) * plan.warps_per_block;
+}
+
+int max_warps_per_block(const DeviceGraphView& g, std::uint32_t efcap) {
+    return (efcap <= kRegBeamCap && g.precision != kFP32 ? kMaxThreads<kBF16, true>
+                                                         : kMaxThreads<kFP32, false>) / 32;
 }
 
 SearchPlan default_plan(const DeviceGraphView& g, std::uint32_t max_ef, bool allow_global) {

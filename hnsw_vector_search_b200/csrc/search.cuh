@@ -124,6 +124,10 @@ std::size_t plan_search(SearchArgs& args, const SearchPlan& plan);
 // can provide global visited tables (global_visited_bytes), used from ef capacity 512 up.
 SearchPlan default_plan(const DeviceGraphView& g, std::uint32_t max_ef, bool allow_global = false);
 
+// The most warps per block a plan of result capacity `efcap` may use on graph `g` (4 for the
+// register-limited BF16 / FP8 kernels of capacity <= 64, else 8); launch_search rejects more.
+int max_warps_per_block(const DeviceGraphView& g, std::uint32_t efcap);
+
 // Warps the launch of `plan` runs (the grid the launcher picks before trimming it to a short
 // batch), and the bytes of global visited tables and epoch counters for `warps` warps of
 // `stride` slots each. A buffer is zeroed once when laid out; it stays valid for every later

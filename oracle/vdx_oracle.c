@@ -227,8 +227,8 @@ vo_index* vo_index_load(const char* path) {
     memcpy(&ix->upper_blocks, h + 72, 8);
     const uint64_t n = ix->n, b0 = 1 + 2 * ix->M, b1 = 1 + ix->M;
     ix->levels = (uint8_t*)malloc(n ? n : 1);
-    ix->layer0 = (uint32_t*)malloc((n * b0 ? n * b0 : 1) * 4);
-    ix->upper = (uint32_t*)malloc((ix->upper_blocks * b1 ? ix->upper_blocks * b1 : 1) * 4);
+    ix->layer0 = (uint32_t*)malloc((n * b0 != 0 ? n * b0 : 1) * 4);
+    ix->upper = (uint32_t*)malloc((ix->upper_blocks * b1 != 0 ? ix->upper_blocks * b1 : 1) * 4);
     ix->upper_at = (uint64_t*)malloc((n ? n : 1) * 8);
     ix->vectors = (float*)malloc((n * ix->dim != 0 ? n * ix->dim : 1) * 4);
     int ok = fread(ix->levels, 1, n, f) == n && fread(ix->layer0, 4, n * b0, f) == n * b0 &&

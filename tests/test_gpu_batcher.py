@@ -87,6 +87,22 @@ def test_autotune_keeps_results(gpu, graph):
 
 
 @pytest.mark.gpu
+def test_autotune_bf16_keeps_block_limit_and_results(gpu, graph):
+    """BF16 kernels of capacity <= 64 run blocks of at most 4 warps (96 registers a thread):
+    the autotuner tries only those, and its plan gives the same rows."""
+    bt = gpu.Batcher(graph, max_queries=200, max_k=10, max_ef=64, precision="bf16")
+    q = integer_matrix(200, 24, seed=19)
+    k = np.full(200, 10, np.uint32)
+    ef = np.full(200, 40, np.uint32)
+    before = bt.run(q, k, ef)
+    timings = bt.autotune(q, k, ef)
+    assert timings and max(t["warps_per_block"] for t in timings) == 4
+    after = bt.run(q, k, ef)
+    for x, y in zip(before, after):
+        np.testing.assert_array_equal(x, y)
+
+
+@pytest.mark.gpu
 def test_batcher_rejects_what_does_not_fit(gpu, graph):
     bt = gpu.Batcher(graph, max_queries=8, max_k=5, max_ef=32)
     q = integer_matrix(9, 24, seed=3)
