@@ -888,7 +888,11 @@ std::size_t plan_search(SearchArgs& a, const SearchPlan& plan) {
     a.off_ap = off;
     off += 32 * 4;
     a.off_hist = off;
-    off += (kHist + kHidden) * 4;
+    if (a.stop_enabled != nullptr || a.trace.truth != nullptr) {
+        // Only the learned stop and its traces read the history ring and network scratch; the
+        // kernel takes both flags from these same arguments, so the layout always matches.
+        off += (kHist + kHidden) * 4;
+    }
     a.warp_bytes = round_up(off, 16);
     return static_cast<std::size_t>(a.warp_bytes) * plan.warps_per_block;
 }
@@ -905,12 +909,12 @@ SearchPlan default_plan(const DeviceGraphView& g, std::uint32_t max_ef, bool all
         cap <<= 1;
     }
     p.efcap = cap;
-    // 16 slots per result entry, at least 2048 for FP32 rows and 1024 for BF16 / FP8 rows: on
-    // the 1M x 128 workload a query visits ~600 nodes at ef = 36 and ~3k at ef = 512. With the
-    // smaller rows the smaller table lets 20 instead of 12 warps reside per SM (2.7 % faster in
-    // BF16 at ef = 36); with FP32 rows it buys no extra warp and only costs filter misses (10 %
-    // slower), measured side by side in one process.
-    std::uint32_t slots = g.precision == 0 ? 2048 : 1024;
+    // 16 slots per result entry, at least 1024: on the 1M x 128 workload a query visits ~600
+    // nodes at ef = 36 and ~3k at ef = 512. The small table costs some filter misses (rows scored
+    // twice) but keeps a warp's layout small: with BF16 / FP8 rows 20 warps reside per SM, with
+    // FP32 rows 16 instead of 12 with a 2048-slot table (and no learned-stop scratch), which
+    // made FP32 at ef = 36 / 64 11.7 % / 7.2 % faster, timed side by side, results identical.
+    std::uint32_t slots = 1024;
     while (slots < 16 * cap && slots < 32768) {
         slots <<= 1;
     }
