@@ -446,7 +446,9 @@ def main():
             "sweep": sweep,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": f"search_kernel ({best})",
+                         "kernel": f"one ordered search call ({best}): search_kernel descent pass, "
+                                   "order_kernel, search_kernel layer-0 pass; CUDA-event time of "
+                                   "the call, traffic of both passes",
                          "algorithmic_bytes_per_launch": algorithmic},
             "cpu_baseline": cpu,
             "e2e": {"value": nq * world * args.steps / e2e_total, "unit": "queries/s",
