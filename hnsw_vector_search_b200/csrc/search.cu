@@ -347,10 +347,13 @@ __global__ void __launch_bounds__(kMaxThreads<P, kRegR>, kLowRegs<P, kRegR> ? 5 
             curd = lane_distance<P, kL2>(q, rows, g.dim, g.row_bytes);
             ++c_du;
             c_rb += g.row_bytes;
+            // cur's first upper block; a move takes the new node's from the candidates' indices,
+            // loaded while their rows are gathered, so a hop waits on one dependent read less.
+            std::uint32_t cur_ua = g.max_level > 0 ? g.upper_at[cur] : 0;
             for (int layer = static_cast<int>(g.max_level); layer >= 1; --layer) {
                 for (std::uint32_t hop = 0; hop <= g.n; ++hop) {
                     const std::uint32_t* block =
-                        g.links_up + static_cast<std::size_t>(g.upper_at[cur] + layer - 1) * g.stride_up;
+                        g.links_up + static_cast<std::size_t>(cur_ua + layer - 1) * g.stride_up;
                     int f = 0;
                     for (std::uint32_t c0 = 0; c0 < g.cap_up; c0 += 32) {
                         const std::uint32_t j = c0 + lane;
@@ -370,9 +373,12 @@ __global__ void __launch_bounds__(kMaxThreads<P, kRegR>, kLowRegs<P, kRegR> ? 5 
                     c_lb += 4ull * (1 + f);
                     float best_d = INFINITY;
                     int best_i = 0x7FFFFFFF;
+                    std::uint32_t best_ua = 0;
                     for (int s0 = 0; s0 < f; s0 += rounds_cap) {
                         const int cnt = min(rounds_cap, f - s0);
                         gather_rows(rows, stride_s, vecs, fresh + s0, cnt, g.row_bytes, shift, lane);
+                        // Candidates sit on this layer, so each has upper blocks (ids < n: checked).
+                        const std::uint32_t ua = lane < cnt ? g.upper_at[fresh[s0 + lane]] : 0u;
                         cp_async_wait<0>();
                         __syncwarp();
                         const float pd = pair_distance<P, kL2>(q, my_row, g.dim, g.row_bytes, half);
@@ -388,9 +394,11 @@ __global__ void __launch_bounds__(kMaxThreads<P, kRegR>, kLowRegs<P, kRegR> ? 5 
                             warp_argmin(d, static_cast<std::uint32_t>(idx), d, bidx);
                             idx = static_cast<int>(bidx);
                         }
+                        const std::uint32_t round_ua = __shfl_sync(kFull, ua, (idx - s0) & 31);
                         if (d < best_d) {
                             best_d = d;
                             best_i = idx;
+                            best_ua = round_ua;
                         }
                         __syncwarp();
                     }
@@ -398,6 +406,7 @@ __global__ void __launch_bounds__(kMaxThreads<P, kRegR>, kLowRegs<P, kRegR> ? 5 
                     c_rb += static_cast<unsigned long long>(f) * g.row_bytes;
                     if (f > 0 && best_d < curd) {
                         cur = fresh[best_i];
+                        cur_ua = best_ua;
                         curd = best_d;
                         __syncwarp();
                     } else {
@@ -653,19 +662,24 @@ __global__ void __launch_bounds__(kMaxThreads<P, kRegR>, kLowRegs<P, kRegR> ? 5 
             const std::uint32_t row32b = g.row32 * 4;
             const std::uint32_t stride32 = padded_row_stride(row32b);
             const int shift32 = chunk_shift(row32b);
-            const int per_round = max(1, min(32, static_cast<int>((a.rows_cap * stride_s) / stride32)));
+            // The walk is over: the visited filter, the link buffers and the row buffer form one
+            // free region [off_hash, off_fresh) (at least one FP32 row: the row area is sized for
+            // it). Two lanes score each row, so a round holds at most 16.
+            unsigned char* const rrows = ws + a.off_hash;
+            const int per_round =
+                max(1, min(16, static_cast<int>((a.off_fresh - a.off_hash) / stride32)));
+            const unsigned char* const my_rrow =
+                rrows + static_cast<std::uint32_t>(min(lane & 15, per_round - 1)) * stride32;
             int rr = 0;
             for (int s0 = 0; s0 < m; s0 += per_round) {
                 const int cnt = min(per_round, m - s0);
-                gather_rows(rows, stride32, reinterpret_cast<const unsigned char*>(g.vectors32),
+                gather_rows(rrows, stride32, reinterpret_cast<const unsigned char*>(g.vectors32),
                             fresh + s0, cnt, row32b, shift32, lane);
                 cp_async_wait<0>();
                 __syncwarp();
                 const bool valid = lane < cnt;
-                float my_d = INFINITY;
-                if (valid) {
-                    my_d = lane_distance<kFP32, kL2>(q, rows + lane * stride32, g.dim, row32b);
-                }
+                const float pd = pair_distance<kFP32, kL2>(q, my_rrow, g.dim, row32b, half);
+                const float my_d = valid ? pd : INFINITY;
                 const std::uint32_t my_id = valid ? fresh[s0 + lane] : kNoId;
                 c_rr += static_cast<unsigned long long>(cnt) * row32b;
                 __syncwarp();
