@@ -34,7 +34,8 @@ __device__ __forceinline__ bool first_visit(std::uint32_t* table, std::uint32_t 
 // Copies `count` rows (ids in `ids`, shared) of `row_bytes` each from `base` into `dst`
 // (shared, rows `dst_stride` bytes apart), 16 bytes per lane per step, and commits them as one
 // cp.async group. `shift` is log2(row_bytes / 16) when that is a power of two up to 32 (several
-// rows per warp-wide step, no division), else -1.
+// rows per warp-wide step, no division), else -1. kL1: copy through L1 (see cp_async16).
+template <bool kL1 = false>
 __device__ __forceinline__ void gather_rows(unsigned char* dst, std::uint32_t dst_stride,
                                             const unsigned char* base, const std::uint32_t* ids,
                                             std::uint32_t count, std::uint32_t row_bytes, int shift,
@@ -47,15 +48,15 @@ __device__ __forceinline__ void gather_rows(unsigned char* dst, std::uint32_t ds
         for (std::uint32_t r0 = 0; r0 < count; r0 += per_step) {
             const std::uint32_t r = r0 + r_in;
             if (r < count) {
-                cp_async16(dst + r * dst_stride + (c << 4),
-                           base + static_cast<std::size_t>(ids[r]) * row_bytes + (c << 4));
+                cp_async16<kL1>(dst + r * dst_stride + (c << 4),
+                                base + static_cast<std::size_t>(ids[r]) * row_bytes + (c << 4));
             }
         }
     } else {
         for (std::uint32_t r = 0; r < count; ++r) {
             const unsigned char* src = base + static_cast<std::size_t>(ids[r]) * row_bytes;
             for (std::uint32_t c = static_cast<std::uint32_t>(lane); c < chunks; c += 32) {
-                cp_async16(dst + r * dst_stride + (c << 4), src + (c << 4));
+                cp_async16<kL1>(dst + r * dst_stride + (c << 4), src + (c << 4));
             }
         }
     }

@@ -33,11 +33,20 @@ __device__ __forceinline__ std::uint32_t smem_addr(const void* p) {
     return static_cast<std::uint32_t>(__cvta_generic_to_shared(p));
 }
 
-// One 16-byte global -> shared copy, bypassing L1 (cp.async.cg). Both addresses 16-aligned.
+// One 16-byte global -> shared copy, bypassing L1 (cp.async.cg), or with kL1 through L1
+// (cp.async.ca: for data many warps of an SM read, like the upper layers' rows). Both addresses
+// 16-aligned.
+template <bool kL1 = false>
 __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_addr(smem_dst)),
-                 "l"(gmem_src)
-                 : "memory");
+    if constexpr (kL1) {
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(smem_addr(smem_dst)),
+                     "l"(gmem_src)
+                     : "memory");
+    } else {
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_addr(smem_dst)),
+                     "l"(gmem_src)
+                     : "memory");
+    }
 }
 __device__ __forceinline__ void cp_async_commit() {
     asm volatile("cp.async.commit_group;\n" ::: "memory");

@@ -341,7 +341,7 @@ __global__ void __launch_bounds__(kMaxThreads<P, kRegR>, kLowRegs<P, kRegR> ? 5 
                 fresh[0] = cur;
             }
             __syncwarp();
-            gather_rows(rows, stride_s, vecs, fresh, 1, g.row_bytes, shift, lane);
+            gather_rows<true>(rows, stride_s, vecs, fresh, 1, g.row_bytes, shift, lane);
             cp_async_wait<0>();
             __syncwarp();
             curd = lane_distance<P, kL2>(q, rows, g.dim, g.row_bytes);
@@ -376,7 +376,8 @@ __global__ void __launch_bounds__(kMaxThreads<P, kRegR>, kLowRegs<P, kRegR> ? 5 
                     std::uint32_t best_ua = 0;
                     for (int s0 = 0; s0 < f; s0 += rounds_cap) {
                         const int cnt = min(rounds_cap, f - s0);
-                        gather_rows(rows, stride_s, vecs, fresh + s0, cnt, g.row_bytes, shift, lane);
+                        gather_rows<true>(rows, stride_s, vecs, fresh + s0, cnt, g.row_bytes, shift,
+                                          lane);
                         // Candidates sit on this layer, so each has upper blocks (ids < n: checked).
                         const std::uint32_t ua = lane < cnt ? g.upper_at[fresh[s0 + lane]] : 0u;
                         cp_async_wait<0>();
