@@ -190,6 +190,15 @@ constexpr bool kLowRegs = kRegR && P != kFP32;
 template <int P, bool kRegR>
 constexpr int kMaxThreads = kLowRegs<P, kRegR> ? 128 : 256;
 
+// pair_distance with the loops of the most common dimension (128, SIFT-like data) unrolled at
+// compile time; any other dimension takes the general loop. Same bits either way.
+template <int P, bool kL2>
+__device__ __forceinline__ float row_distance(const float* q, const unsigned char* row,
+                                              std::uint32_t dim, std::uint32_t row_bytes, int half) {
+    return dim == 128 ? pair_distance<P, kL2, 128>(q, row, dim, row_bytes, half)
+                      : pair_distance<P, kL2>(q, row, dim, row_bytes, half);
+}
+
 // kRegR: R in registers (RegBeam, result capacity up to 64) instead of shared memory.
 template <int P, bool kL2, bool kRegR>
 __global__ void __launch_bounds__(kMaxThreads<P, kRegR>, kLowRegs<P, kRegR> ? 5 : 0)
@@ -382,7 +391,7 @@ __global__ void __launch_bounds__(kMaxThreads<P, kRegR>, kLowRegs<P, kRegR> ? 5 
                         const std::uint32_t ua = lane < cnt ? g.upper_at[fresh[s0 + lane]] : 0u;
                         cp_async_wait<0>();
                         __syncwarp();
-                        const float pd = pair_distance<P, kL2>(q, my_row, g.dim, g.row_bytes, half);
+                        const float pd = row_distance<P, kL2>(q, my_row, g.dim, g.row_bytes, half);
                         float d = INFINITY;
                         int idx = 0x7FFFFFFF;
                         if (lane < cnt) {
@@ -546,7 +555,7 @@ __global__ void __launch_bounds__(kMaxThreads<P, kRegR>, kLowRegs<P, kRegR> ? 5 
                 cp_async_wait<0>();
                 __syncwarp();
                 const bool valid = lane < cnt;
-                const float pd = pair_distance<P, kL2>(q, my_row, g.dim, g.row_bytes, half);
+                const float pd = row_distance<P, kL2>(q, my_row, g.dim, g.row_bytes, half);
                 const float my_d = valid ? pd : INFINITY;
                 const std::uint32_t my_id = valid ? fresh[s0 + lane] : kNoId;
                 c_d0 += cnt;
@@ -679,7 +688,7 @@ __global__ void __launch_bounds__(kMaxThreads<P, kRegR>, kLowRegs<P, kRegR> ? 5 
                 cp_async_wait<0>();
                 __syncwarp();
                 const bool valid = lane < cnt;
-                const float pd = pair_distance<kFP32, kL2>(q, my_rrow, g.dim, row32b, half);
+                const float pd = row_distance<kFP32, kL2>(q, my_rrow, g.dim, row32b, half);
                 const float my_d = valid ? pd : INFINITY;
                 const std::uint32_t my_id = valid ? fresh[s0 + lane] : kNoId;
                 c_rr += static_cast<unsigned long long>(cnt) * row32b;
