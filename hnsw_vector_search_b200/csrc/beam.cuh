@@ -31,6 +31,42 @@ __device__ __forceinline__ bool first_visit(std::uint32_t* table, std::uint32_t 
     return true;
 }
 
+// The same contract with the table read as 4-slot buckets (16 bytes, one shared-memory load):
+// an id lives in the first bucket of its sequence that had an empty slot when it was inserted,
+// and slots only fill, so a lookup that meets a bucket with an empty slot and without the id
+// knows the id is new. Most lookups read one bucket, where slot-by-slot linear probing walked
+// the table's clusters one atomic at a time. A lane that loses a slot to another lane's CAS
+// reads the bucket again; a lane that meets kProbes / 4 full buckets reports "unvisited".
+__device__ __forceinline__ bool first_visit_bucket(std::uint32_t* table, std::uint32_t mask,
+                                                   std::uint32_t id) {
+    std::uint32_t b = (id * 2654435761u) & mask & ~3u;
+    int full = 0;
+#pragma unroll 1
+    for (int step = 0; step < 2 * kProbes; ++step) {
+        const uint4 s = *reinterpret_cast<const uint4*>(table + b);
+        if (s.x == id || s.y == id || s.z == id || s.w == id) {
+            return false;
+        }
+        const std::uint32_t e = s.x == kNoId ? 0u : s.y == kNoId ? 1u : s.z == kNoId ? 2u
+                                : s.w == kNoId ? 3u : 4u;
+        if (e < 4) {
+            const std::uint32_t old = atomicCAS(table + b + e, kNoId, id);
+            if (old == kNoId) {
+                return true;
+            }
+            if (old == id) {
+                return false;
+            }
+            continue;  // another lane took the slot: read the bucket again
+        }
+        if (++full >= kProbes / 4) {
+            return true;
+        }
+        b = (b + 4) & mask;
+    }
+    return true;
+}
+
 // Copies `count` rows (ids in `ids`, shared) of `row_bytes` each from `base` into `dst`
 // (shared, rows `dst_stride` bytes apart), 16 bytes per lane per step, and commits them as one
 // cp.async group. `shift` is log2(row_bytes / 16) when that is a power of two up to 32 (several

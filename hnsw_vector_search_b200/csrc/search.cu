@@ -20,7 +20,8 @@
 // memory, all rows of a round in flight together; the link block of the next likely expansion
 // (the second-best unexpanded entry) is prefetched while the current one is processed.
 //
-// The visited set is a per-warp shared-memory open-addressing hash. It never reports an
+// The visited set is a per-warp shared-memory open-addressing hash of 4-slot buckets (one 16-byte
+// load per bucket, first_visit_bucket). It never reports an
 // unvisited node as visited. If its probe limit is reached it reports "unvisited" and the node is
 // scored again; the merge then drops the copy already in R (equal distance and id), so results
 // stay exact and the only cost is the extra row read (counted in kStatDuplicates).
@@ -232,7 +233,7 @@ __global__ void __launch_bounds__(kMaxThreads<P, kRegR>, kLowRegs<P, kRegR> ? 5 
     const std::uint32_t gmask = a.gslots - 1;
     const auto visit = [&](std::uint32_t id, std::uint32_t epoch) {
         return gtable != nullptr ? first_visit_global(gtable, gmask, id, epoch)
-                                 : first_visit(table, hmask, id);
+                                 : first_visit_bucket(table, hmask, id);
     };
     // Two lanes score each row (pair_distance), so a round stages at most 16 rows.
     const int rounds_cap = static_cast<int>(a.rows_cap < 16 ? a.rows_cap : 16);
