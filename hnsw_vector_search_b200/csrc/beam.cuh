@@ -168,12 +168,16 @@ __device__ __forceinline__ int reg_first_unexpanded(const RegBeam& b, int from, 
     return m1 != 0 ? 32 + __ffs(m1) - 1 : r;
 }
 
-// merge_round (common.cuh) over the registers, with the same steps and so the same result: the
-// full-list admission test, each candidate's position `lo` by the same binary search (probes
-// read by shuffles), the duplicate test at `lo`, the rank among admitted candidates, entries at
-// index i moved up by the number of admitted positions <= i, and everything at ef or beyond
-// dropped. The new R is scattered into the shared-memory mirror (rd, rid) and read back into
-// the registers. Returns the lowest position a candidate was kept at (0x7FFFFFFF if none).
+// merge_round (common.cuh) over the registers, with the same result: the full-list admission
+// test, each candidate's position `lo` (the number of entries closer than it), the duplicate
+// test (its id already in R), the rank among admitted candidates, entries at index i moved up by
+// the number of admitted positions <= i, and everything at ef or beyond dropped. The candidates
+// that pass the admission test are taken one at a time, broadcast to the warp: every lane
+// compares them with its two entries, and two ballots count `lo` — no binary search, so a round
+// costs a few shuffles and votes per surviving candidate (in a full list usually two or three
+// of the ~13 scored). The new R is scattered into the shared-memory mirror (rd, rid) and read
+// back into the registers. Returns the lowest position a candidate was kept at (0x7FFFFFFF if
+// none).
 __device__ __forceinline__ int reg_merge_round(RegBeam& b, float* rd, std::uint32_t* rid, int& r,
                                                int ef, float my_d, std::uint32_t my_id, bool valid,
                                                int lane, unsigned long long& dups) {
@@ -182,57 +186,51 @@ __device__ __forceinline__ int reg_merge_round(RegBeam& b, float* rd, std::uint3
         const std::uint32_t wi = reg_id(b, r - 1) & kIdMask;
         valid = valid && closer(my_d, my_id, wd, wi);
     }
-    int lo = 0;
-    int hi = valid ? r : 0;
-    while (__any_sync(kFull, lo < hi)) {
-        const int mid = (lo + hi) >> 1;
-        const int src = mid & 31;
-        const float m0 = __shfl_sync(kFull, b.d0, src);
-        const float m1 = __shfl_sync(kFull, b.d1, src);
-        const std::uint32_t j0 = __shfl_sync(kFull, b.i0, src);
-        const std::uint32_t j1 = __shfl_sync(kFull, b.i1, src);
-        if (lo < hi) {
-            const float dm = mid < 32 ? m0 : m1;
-            const std::uint32_t im = (mid < 32 ? j0 : j1) & kIdMask;
-            if (dm < my_d || (dm == my_d && im < my_id)) {
-                lo = mid + 1;
-            } else {
-                hi = mid;
-            }
-        }
-    }
-    const std::uint32_t a0 = __shfl_sync(kFull, b.i0, lo & 31);
-    const std::uint32_t a1 = __shfl_sync(kFull, b.i1, lo & 31);
-    const bool adm = valid && !(lo < r && ((lo < 32 ? a0 : a1) & kIdMask) == my_id);
-    const std::uint32_t dupmask = __ballot_sync(kFull, valid && !adm);
-    if (lane == 0) {
-        dups += __popc(dupmask);
-    }
-    const std::uint32_t am = __ballot_sync(kFull, adm);
-    if (am == 0) {
+    const std::uint32_t vm = __ballot_sync(kFull, valid);
+    if (vm == 0) {
         return 0x7FFFFFFF;
     }
+    // Entries at r and beyond hold (+inf, kNoId): never closer than a candidate, never equal.
+    const std::uint32_t e0 = b.i0 & kIdMask;
+    const std::uint32_t e1 = b.i1 & kIdMask;
+    const bool live0 = lane < r;
+    const bool live1 = 32 + lane < r;
+    std::uint32_t am = 0;
     int rank = 0;
     int s0 = 0;
     int s1 = 0;
-    for (std::uint32_t m = am; m != 0; m &= m - 1) {
+    int lo = 0;
+    for (std::uint32_t m = vm; m != 0; m &= m - 1) {
         const int j = __ffs(m) - 1;
         const float dj = __shfl_sync(kFull, my_d, j);
         const std::uint32_t ij = __shfl_sync(kFull, my_id, j);
-        const int lj = __shfl_sync(kFull, lo, j);
-        rank += (adm && closer(dj, ij, my_d, my_id)) ? 1 : 0;
-        s0 += lj <= lane ? 1 : 0;
-        s1 += lj <= 32 + lane ? 1 : 0;
+        const bool dup = __any_sync(kFull, (live0 && e0 == ij) || (live1 && e1 == ij));
+        if (!dup) {
+            const int lj = __popc(__ballot_sync(kFull, live0 && closer(b.d0, e0, dj, ij))) +
+                           __popc(__ballot_sync(kFull, live1 && closer(b.d1, e1, dj, ij)));
+            am |= 1u << j;
+            rank += closer(dj, ij, my_d, my_id) ? 1 : 0;
+            s0 += lj <= lane ? 1 : 0;
+            s1 += lj <= 32 + lane ? 1 : 0;
+            lo = lane == j ? lj : lo;
+        }
     }
+    if (lane == 0) {
+        dups += __popc(vm & ~am);
+    }
+    if (am == 0) {
+        return 0x7FFFFFFF;
+    }
+    const bool adm = ((am >> lane) & 1u) != 0;
     const int p0 = lane + s0;
     const int p1 = 32 + lane + s1;
     const int newpos = lo + rank;
     const bool keep = adm && newpos < ef;
-    if (lane < r && p0 < ef) {
+    if (live0 && p0 < ef) {
         rd[p0] = b.d0;
         rid[p0] = b.i0;
     }
-    if (32 + lane < r && p1 < ef) {
+    if (live1 && p1 < ef) {
         rd[p1] = b.d1;
         rid[p1] = b.i1;
     }
