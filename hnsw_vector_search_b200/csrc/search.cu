@@ -33,6 +33,7 @@
 
 #include <cmath>
 #include <cstdint>
+#include <vector>
 
 #include "beam.cuh"
 #include "common.cuh"
@@ -826,6 +827,73 @@ __global__ void __launch_bounds__(kOrderThreads) order_kernel(const SearchArgs a
 
 thread_local int g_last_kernels = 1;
 
+// Host-side launch bookkeeping, cached per thread so that a repeated search launch makes no
+// attribute or occupancy query (each costs microseconds on the host, and the device waits for
+// the launch meanwhile): the dynamic shared-memory limit set on each kernel per device (only
+// ever raised, so a launch never lowers it under another thread's larger launch), and the
+// resident blocks of each (kernel, device, block size, shared memory) shape.
+struct SmemLimit {
+    const void* kernel;
+    int device;
+    std::size_t bytes;
+};
+struct Residency {
+    const void* kernel;
+    int device;
+    int threads;
+    std::size_t smem;
+    int blocks;
+};
+thread_local std::vector<SmemLimit> g_smem_limits;
+thread_local std::vector<Residency> g_residency;
+
+cudaError_t raise_smem_limit(const void* kernel, int device, std::size_t smem) {
+    for (SmemLimit& l : g_smem_limits) {
+        if (l.kernel == kernel && l.device == device) {
+            if (smem <= l.bytes) {
+                return cudaSuccess;
+            }
+            const cudaError_t err = cudaFuncSetAttribute(
+                kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+            if (err == cudaSuccess) {
+                l.bytes = smem;
+            }
+            return err;
+        }
+    }
+    const cudaError_t err =
+        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (err == cudaSuccess) {
+        g_smem_limits.push_back({kernel, device, smem});
+    }
+    return err;
+}
+
+// Blocks of `threads` threads and `smem` bytes that the device holds at once (SMs x per SM).
+cudaError_t resident_blocks(const void* kernel, int device, int threads, std::size_t smem, int& blocks) {
+    for (const Residency& r : g_residency) {
+        if (r.kernel == kernel && r.device == device && r.threads == threads && r.smem == smem) {
+            blocks = r.blocks;
+            return cudaSuccess;
+        }
+    }
+    int sms = 0;
+    cudaError_t err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (err != cudaSuccess) {
+        return err;
+    }
+    int per_sm = 0;
+    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
+    if (err != cudaSuccess) {
+        return err;
+    }
+    blocks = sms * (per_sm > 0 ? per_sm : 1);
+    if (g_residency.size() < 64) {
+        g_residency.push_back({kernel, device, threads, smem, blocks});
+    }
+    return cudaSuccess;
+}
+
 template <int P, bool kL2, bool kRegR>
 cudaError_t launch_typed(SearchArgs& args, const SearchPlan& plan, std::size_t smem,
                          cudaStream_t stream) {
@@ -833,24 +901,22 @@ cudaError_t launch_typed(SearchArgs& args, const SearchPlan& plan, std::size_t s
     if (plan.warps_per_block < 1 || plan.warps_per_block * 32 > kMaxThreads<P, kRegR>) {
         return cudaErrorInvalidValue;  // a plan beyond max_warps_per_block
     }
-    cudaError_t err =
-        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    int device = 0;
+    cudaError_t err = cudaGetDevice(&device);
+    if (err != cudaSuccess) {
+        return err;
+    }
+    err = raise_smem_limit(reinterpret_cast<const void*>(kernel), device, smem);
     if (err != cudaSuccess) {
         return err;
     }
     const int threads = plan.warps_per_block * 32;
     int blocks = plan.blocks;
     if (blocks <= 0) {
-        int device = 0;
-        cudaGetDevice(&device);
-        int sms = 0;
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-        int per_sm = 0;
-        err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
+        err = resident_blocks(reinterpret_cast<const void*>(kernel), device, threads, smem, blocks);
         if (err != cudaSuccess) {
             return err;
         }
-        blocks = sms * (per_sm > 0 ? per_sm : 1);
     }
     const std::uint32_t nq = args.nq;
     const std::uint32_t needed = (nq + plan.warps_per_block - 1) / plan.warps_per_block;
@@ -969,14 +1035,17 @@ std::uint32_t search_warps(SearchArgs& args, const SearchPlan& plan) {
     const std::size_t smem = plan_search(args, plan);
     int device = 0;
     cudaGetDevice(&device);
-    int sms = 0;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     const int threads = plan.warps_per_block * 32;
-    const auto per_sm_of = [&](const void* kernel) {
-        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-        int per_sm = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
-        return per_sm > 0 ? per_sm : 1;
+    // The grid launch_typed will pick for this kernel (same cached bookkeeping).
+    const auto grid_of = [&](const void* kernel) {
+        int blocks = 0;
+        if (raise_smem_limit(kernel, device, smem) != cudaSuccess ||
+            resident_blocks(kernel, device, threads, smem, blocks) != cudaSuccess) {
+            int sms = 0;
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+            return sms;
+        }
+        return blocks;
     };
     const bool l2 = args.g.metric == 0;
     // The kernel launch_search will pick (the register-beam variants for small capacities).
@@ -1002,8 +1071,7 @@ std::uint32_t search_warps(SearchArgs& args, const SearchPlan& plan) {
                                : reinterpret_cast<const void*>(&search_kernel<kFP8, false, false>));
             break;
     }
-    const int per_sm = per_sm_of(kernel);
-    return static_cast<std::uint32_t>(sms * per_sm * plan.warps_per_block);
+    return static_cast<std::uint32_t>(grid_of(kernel) * plan.warps_per_block);
 }
 
 std::size_t global_visited_bytes(std::uint32_t stride, std::uint32_t warps) {
