@@ -257,8 +257,11 @@ cudaError_t launch_bruteforce_exact(const BruteArgs& a, cudaStream_t stream) {
     }
     const bool l2 = a.base.metric == 0;
     auto* kernel = l2 ? &bf_exact_kernel<true> : &bf_exact_kernel<false>;
-    cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           static_cast<int>(smem));
+    int device = 0;
+    cudaError_t err = cudaGetDevice(&device);
+    if (err == cudaSuccess) {
+        err = raise_smem_limit(reinterpret_cast<const void*>(kernel), device, smem);
+    }
     if (err != cudaSuccess) {
         return err;
     }

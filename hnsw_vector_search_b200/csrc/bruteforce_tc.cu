@@ -1017,8 +1017,13 @@ cudaError_t launch_bruteforce_tc(const BruteArgs& a, const TcBase& b, void* work
     p.off_b = pl.off_b;
     p.off_lists = pl.off_lists;
     p.off_bar = pl.off_bar;
-    err = cudaFuncSetAttribute(bf_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               static_cast<int>(pl.smem));
+    {
+        int device = 0;
+        err = cudaGetDevice(&device);
+        if (err == cudaSuccess) {
+            err = raise_smem_limit(reinterpret_cast<const void*>(&bf_tc_kernel), device, pl.smem);
+        }
+    }
     if (err != cudaSuccess) {
         return err;
     }

@@ -29,6 +29,13 @@ constexpr std::uint32_t kFull = 0xFFFFFFFFu;
 
 enum : int { kFP32 = 0, kBF16 = 1, kFP8 = 2 };
 
+// Raises `kernel`'s dynamic shared-memory limit on `device` to at least `smem` bytes and never
+// lowers it: the limit belongs to the device's context and is shared by every host thread, so a
+// launch that set it to its own smaller size could make another thread's larger launch fail.
+// Every kernel launched with a varying dynamic shared-memory size sets it through here.
+// Defined in search.cu.
+cudaError_t raise_smem_limit(const void* kernel, int device, std::size_t smem);
+
 __device__ __forceinline__ std::uint32_t smem_addr(const void* p) {
     return static_cast<std::uint32_t>(__cvta_generic_to_shared(p));
 }

@@ -33,6 +33,7 @@
 
 #include <cmath>
 #include <cstdint>
+#include <mutex>
 #include <vector>
 
 #include "beam.cuh"
@@ -827,11 +828,12 @@ __global__ void __launch_bounds__(kOrderThreads) order_kernel(const SearchArgs a
 
 thread_local int g_last_kernels = 1;
 
-// Host-side launch bookkeeping, cached per thread so that a repeated search launch makes no
-// attribute or occupancy query (each costs microseconds on the host, and the device waits for
-// the launch meanwhile): the dynamic shared-memory limit set on each kernel per device (only
-// ever raised, so a launch never lowers it under another thread's larger launch), and the
-// resident blocks of each (kernel, device, block size, shared memory) shape.
+// Host-side launch bookkeeping. The dynamic shared-memory limit of each kernel is a property of
+// the device's context, shared by every host thread: it is only ever raised, under a process-wide
+// lock, so no launch can lower it under another thread's larger launch (which then fails with
+// "invalid argument"); each thread remembers the limits it has seen, which stay valid since they
+// only grow. The resident blocks of each (kernel, device, block size, shared memory) shape are
+// cached per thread. A repeated launch makes no attribute or occupancy query.
 struct SmemLimit {
     const void* kernel;
     int device;
@@ -844,30 +846,11 @@ struct Residency {
     std::size_t smem;
     int blocks;
 };
-thread_local std::vector<SmemLimit> g_smem_limits;
+std::mutex g_smem_mutex;
+std::vector<SmemLimit> g_smem_limits;              // the limits set, process-wide
+thread_local std::vector<SmemLimit> g_smem_seen;   // limits this thread knows are in place
 thread_local std::vector<Residency> g_residency;
 
-cudaError_t raise_smem_limit(const void* kernel, int device, std::size_t smem) {
-    for (SmemLimit& l : g_smem_limits) {
-        if (l.kernel == kernel && l.device == device) {
-            if (smem <= l.bytes) {
-                return cudaSuccess;
-            }
-            const cudaError_t err = cudaFuncSetAttribute(
-                kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-            if (err == cudaSuccess) {
-                l.bytes = smem;
-            }
-            return err;
-        }
-    }
-    const cudaError_t err =
-        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-    if (err == cudaSuccess) {
-        g_smem_limits.push_back({kernel, device, smem});
-    }
-    return err;
-}
 
 // Blocks of `threads` threads and `smem` bytes that the device holds at once (SMs x per SM).
 cudaError_t resident_blocks(const void* kernel, int device, int threads, std::size_t smem, int& blocks) {
@@ -955,6 +938,43 @@ cudaError_t launch_typed(SearchArgs& args, const SearchPlan& plan, std::size_t s
 }
 
 }  // namespace
+
+cudaError_t raise_smem_limit(const void* kernel, int device, std::size_t smem) {
+    for (const SmemLimit& l : g_smem_seen) {
+        if (l.kernel == kernel && l.device == device && smem <= l.bytes) {
+            return cudaSuccess;
+        }
+    }
+    const std::scoped_lock lock(g_smem_mutex);
+    SmemLimit* entry = nullptr;
+    for (SmemLimit& l : g_smem_limits) {
+        if (l.kernel == kernel && l.device == device) {
+            entry = &l;
+        }
+    }
+    if (entry == nullptr || smem > entry->bytes) {
+        const cudaError_t err = cudaFuncSetAttribute(
+            kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+        if (err != cudaSuccess) {
+            return err;
+        }
+        if (entry == nullptr) {
+            g_smem_limits.push_back({kernel, device, smem});
+            entry = &g_smem_limits.back();
+        } else {
+            entry->bytes = smem;
+        }
+    }
+    const SmemLimit seen = *entry;
+    for (SmemLimit& l : g_smem_seen) {
+        if (l.kernel == kernel && l.device == device) {
+            l.bytes = seen.bytes;
+            return cudaSuccess;
+        }
+    }
+    g_smem_seen.push_back(seen);
+    return cudaSuccess;
+}
 
 std::size_t plan_search(SearchArgs& a, const SearchPlan& plan) {
     const DeviceGraphView& g = a.g;

@@ -124,3 +124,25 @@ def test_tensor_core_matches_reference(gpu, orc):
     b = ref.search_batch(queries, 10)
     np.testing.assert_array_equal(a[0], b[0])
     np.testing.assert_array_equal(a[1].view(np.uint32), b[1].view(np.uint32))
+
+
+@pytest.mark.parametrize("method", METHODS)
+def test_concurrent_searches_with_different_k(gpu, method):
+    """BruteForceIndex::search is const and safe from several threads; threads with k 1, 10 and
+    40 launch with different shared-memory sizes on one device, and every result equals the same
+    search run alone."""
+    from concurrent.futures import ThreadPoolExecutor
+    if not method_available(gpu, method):
+        pytest.skip(f"{method} brute force is not available on this device")
+    base = integer_matrix(20_000, 64, 5)
+    queries = integer_matrix(256, 64, 6)
+    bf = gpu.BruteForceIndex(64)
+    bf.add(base)
+    ks = [1, 10, 40]
+    want = {k: bf.search_batch(queries, k, method=method) for k in ks}
+    with ThreadPoolExecutor(max_workers=3) as pool:
+        jobs = [(k, pool.submit(bf.search_batch, queries, k, method)) for _ in range(5) for k in ks]
+        for k, job in jobs:
+            got = job.result()
+            np.testing.assert_array_equal(got[0], want[k][0])
+            np.testing.assert_array_equal(got[1].view(np.uint32), want[k][1].view(np.uint32))

@@ -103,6 +103,22 @@ def test_batch_equals_single_searches(gpu, tmp_path):
             assert one == [(float(d[q, i]), int(ids[q, i])) for i in range(c[q])]
 
 
+def test_concurrent_searches_with_different_layouts(gpu, small_l2):
+    """search_batch is safe from several threads at once (include/vecdex/hnsw.hpp:58-62 of the
+    reference). Threads searching at ef 16 / 64 / 128 / 300 launch the kernel with different
+    shared-memory layouts on one device; every result equals the same search run alone."""
+    from concurrent.futures import ThreadPoolExecutor
+    path, _, queries = small_l2
+    ix = gpu.HnswIndex.load(path)
+    q = queries[:300]
+    efs = [16, 64, 128, 300]
+    want = {ef: ix.search_batch(q, 10, ef) for ef in efs}
+    with ThreadPoolExecutor(max_workers=4) as pool:
+        jobs = [(ef, pool.submit(ix.search_batch, q, 10, ef)) for _ in range(6) for ef in efs]
+        for ef, job in jobs:
+            assert_same(job.result(), want[ef], f"ef {ef}")
+
+
 def test_exact_when_ef_covers_every_node(gpu, orc):
     base = uniform_matrix(300, 8, 1)
     queries = uniform_matrix(20, 8, 2)
