@@ -55,27 +55,45 @@ __device__ __forceinline__ void report(std::uint32_t* status, std::uint32_t code
 
 // The same filter in global memory, for large ef (a per-warp table too big for shared memory):
 // 64-bit slots hold (query epoch << 32 | id); a slot whose epoch is not the current query's is
-// empty, so the table never needs clearing between queries. Only this warp's lanes write its
-// table, so a claim can be lost only to a lane of the same warp writing the current epoch, which
-// ends the inner loop: every loop is bounded.
+// empty, so the table never needs clearing between queries. Like first_visit_bucket the table
+// is read as 4-slot buckets (32 bytes, two 16-byte L2 loads): an id lives in the first bucket of
+// its sequence that had an empty slot when it was inserted, and within a query slots only fill.
+// Only this warp's lanes write its table, so a claimed slot is lost only to a lane of the same
+// warp (then the bucket is read again); a lane that meets kProbes / 4 full buckets reports
+// "unvisited". Every loop is bounded.
 __device__ __forceinline__ bool first_visit_global(unsigned long long* table, std::uint32_t mask,
                                                    std::uint32_t id, std::uint32_t epoch) {
     const unsigned long long key = (static_cast<unsigned long long>(epoch) << 32) | id;
-    std::uint32_t h = (id * 2654435761u) & mask;
+    std::uint32_t b = (id * 2654435761u) & mask & ~3u;
+    int full = 0;
 #pragma unroll 1
-    for (int p = 0; p < kProbes; ++p) {
-        unsigned long long old = __ldcg(table + h);
-        while (static_cast<std::uint32_t>(old >> 32) != epoch) {
-            const unsigned long long prev = atomicCAS(table + h, old, key);
+    for (int step = 0; step < 2 * kProbes; ++step) {
+        const ulonglong2 lo = __ldcg(reinterpret_cast<const ulonglong2*>(table + b));
+        const ulonglong2 hi = __ldcg(reinterpret_cast<const ulonglong2*>(table + b + 2));
+        const unsigned long long v[4] = {lo.x, lo.y, hi.x, hi.y};
+        if (v[0] == key || v[1] == key || v[2] == key || v[3] == key) {
+            return false;
+        }
+        int e = 4;
+#pragma unroll
+        for (int i = 3; i >= 0; --i) {
+            e = static_cast<std::uint32_t>(v[i] >> 32) != epoch ? i : e;
+        }
+        if (e < 4) {
+            const unsigned long long old = e == 0 ? v[0] : e == 1 ? v[1] : e == 2 ? v[2] : v[3];
+            const unsigned long long prev = atomicCAS(table + b + e, old, key);
             if (prev == old) {
                 return true;
             }
-            old = prev;
+            if (prev == key) {
+                return false;
+            }
+            continue;  // another lane took the slot: read the bucket again
         }
-        if (old == key) {
-            return false;
+        if (++full >= kProbes / 4) {
+            return true;
         }
-        h = (h + 1) & mask;
+        b = (b + 4) & mask;
     }
     return true;
 }
