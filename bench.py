@@ -373,11 +373,13 @@ def main():
         return total
 
     results = {}
+    kernels_by_mode = {}  # kernels one timed device step launched, per mode
     with Clocks(local) as clocks:
         for name, o in modes:
             ef = points[name][0]
             total = timed(ef, o, args.steps, args.warmup)
             torch.cuda.synchronize()
+            kernels_by_mode[name] = int(v.lib().vdx_search_kernels_last())
             st = work[16:16 + 2 * 10].cpu().numpy().view(np.uint64)
             results[name] = {"ef": ef, "recall": points[name][1], "seconds": total,
                              "qps": nq * world * args.steps / total, "stats": st.tolist()}
@@ -425,7 +427,8 @@ def main():
     if pg is not None:
         pg.barrier()
     if rank == 0:
-        kernels_per_step = int(v.lib().vdx_search_kernels_last())  # the e2e calls' launches
+        kernels_per_step = kernels_by_mode[best]  # one timed device step's launches
+        e2e_kernels = int(v.lib().vdx_search_kernels_last())  # one end-to-end call's launches
         line = {
             "metric": METRIC, "value": r["qps"], "unit": "queries/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
@@ -454,7 +457,8 @@ def main():
             "e2e": {"value": nq * world * args.steps / e2e_total, "unit": "queries/s",
                     "h2d_bytes_per_step": int(queries.nbytes),
                     "d2h_bytes_per_step": int(nq * K * 8 + nq * 4),
-                    "api": "HnswIndex.search_batch(page-locked queries, out=page-locked arrays)"},
+                    "api": "HnswIndex.search_batch(page-locked queries, out=page-locked arrays)",
+                    "gpu_launches_per_call": e2e_kernels},
             "gpu_launches": args.steps * kernels_per_step,
             "clocks": clock_summary,
             "bruteforce": brute,
