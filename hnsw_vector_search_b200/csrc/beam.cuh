@@ -178,9 +178,10 @@ __device__ __forceinline__ int reg_first_unexpanded(const RegBeam& b, int from, 
 // of the ~13 scored). The new R is scattered into the shared-memory mirror (rd, rid) and read
 // back into the registers. Returns the lowest position a candidate was kept at (0x7FFFFFFF if
 // none).
+template <typename Count>
 __device__ __forceinline__ int reg_merge_round(RegBeam& b, float* rd, std::uint32_t* rid, int& r,
                                                int ef, float my_d, std::uint32_t my_id, bool valid,
-                                               int lane, unsigned long long& dups) {
+                                               int lane, Count& dups) {
     if (r >= ef) {
         const float wd = reg_d(b, r - 1);
         const std::uint32_t wi = reg_id(b, r - 1) & kIdMask;

@@ -485,9 +485,10 @@ constexpr std::uint32_t kIdMask = 0x7FFFFFFFu;
 // Merges up to 32 scored candidates (lane j holds candidate j when `valid`) into the sorted list
 // R[0, r) of capacity ef: R = top-ef(R + candidates), candidates equal to an entry of R dropped.
 // Returns the lowest position a candidate was written to (or INT_MAX).
+template <typename Count>
 __device__ __forceinline__ int merge_round(float* rd, std::uint32_t* rid, int& r, int ef,
                                            float my_d, std::uint32_t my_id, bool valid,
-                                           int* ap, int lane, unsigned long long& dups) {
+                                           int* ap, int lane, Count& dups) {
     // A full list admits only candidates that beat its worst entry.
     if (valid && r >= ef) {
         valid = closer(my_d, my_id, rd[r - 1], rid[r - 1] & kIdMask);

@@ -270,8 +270,12 @@ __global__ void __launch_bounds__(kMaxThreads<P, kRegR>, kLowRegs<P, kRegR> ? 5 
         rows + static_cast<std::uint32_t>(min(lane & 15, rounds_cap - 1)) * stride_s;
     const int half = lane >> 4;
 
-    unsigned long long c_exp = 0, c_d0 = 0, c_du = 0, c_lb = 0, c_rb = 0, c_rr = 0, c_dup = 0,
-                       c_pf = 0, c_q = 0, c_stop = 0;
+    // Launch statistics, per warp in 32 bits (a warp's counts stay far below 2^32; the byte
+    // counters are derived from them when flushed): expansions, layer-0 / upper-layer distance
+    // evaluations, link-block words read, re-rank rows, duplicates, prefetch hits, queries,
+    // learned stops.
+    std::uint32_t c_exp = 0, c_d0 = 0, c_du = 0, c_lw = 0, c_rr = 0, c_dup = 0, c_pf = 0, c_q = 0,
+                  c_stop = 0;
 
     for (;;) {
         std::uint32_t qi = 0;
@@ -381,7 +385,6 @@ __global__ void __launch_bounds__(kMaxThreads<P, kRegR>, kLowRegs<P, kRegR> ? 5 
             __syncwarp();
             curd = lane_distance<P, kL2>(q, rows, g.dim, g.row_bytes);
             ++c_du;
-            c_rb += g.row_bytes;
             // cur's first upper block; a move takes the new node's from the candidates' indices,
             // loaded while their rows are gathered, so a hop waits on one dependent read less.
             std::uint32_t cur_ua = g.max_level > 0 ? g.upper_at[cur] : 0;
@@ -405,7 +408,7 @@ __global__ void __launch_bounds__(kMaxThreads<P, kRegR>, kLowRegs<P, kRegR> ? 5 
                         f += __popc(m);
                     }
                     __syncwarp();
-                    c_lb += 4ull * (1 + f);
+                    c_lw += 1 + f;
                     float best_d = INFINITY;
                     int best_i = 0x7FFFFFFF;
                     std::uint32_t best_ua = 0;
@@ -439,7 +442,6 @@ __global__ void __launch_bounds__(kMaxThreads<P, kRegR>, kLowRegs<P, kRegR> ? 5 
                         __syncwarp();
                     }
                     c_du += f;
-                    c_rb += static_cast<unsigned long long>(f) * g.row_bytes;
                     if (f > 0 && best_d < curd) {
                         cur = fresh[best_i];
                         cur_ua = best_ua;
@@ -574,7 +576,7 @@ __global__ void __launch_bounds__(kMaxThreads<P, kRegR>, kLowRegs<P, kRegR> ? 5 
                 f += __popc(m);
             }
             __syncwarp();
-            c_lb += 4ull * (1 + count);
+            c_lw += 1 + count;
             for (int s0 = 0; s0 < f; s0 += rounds_cap) {
                 const int cnt = min(rounds_cap, f - s0);
                 gather_rows(rows, stride_s, vecs, fresh + s0, cnt, g.row_bytes, shift, lane);
@@ -585,7 +587,6 @@ __global__ void __launch_bounds__(kMaxThreads<P, kRegR>, kLowRegs<P, kRegR> ? 5 
                 const float my_d = valid ? pd : INFINITY;
                 const std::uint32_t my_id = valid ? fresh[s0 + lane] : kNoId;
                 c_d0 += cnt;
-                c_rb += static_cast<unsigned long long>(cnt) * g.row_bytes;
                 __syncwarp();
                 if (s0 + rounds_cap >= f) {
                     // Last round: the next expansion is the closer of R's first unexpanded entry
@@ -717,7 +718,7 @@ __global__ void __launch_bounds__(kMaxThreads<P, kRegR>, kLowRegs<P, kRegR> ? 5 
                 const float pd = row_distance<kFP32, kL2>(q, my_rrow, g.dim, row32b, half);
                 const float my_d = valid ? pd : INFINITY;
                 const std::uint32_t my_id = valid ? fresh[s0 + lane] : kNoId;
-                c_rr += static_cast<unsigned long long>(cnt) * row32b;
+                c_rr += cnt;
                 __syncwarp();
                 // Build the re-ranked list in R's storage from scratch: the candidates' ids are
                 // safe in `fresh`.
@@ -760,16 +761,17 @@ __global__ void __launch_bounds__(kMaxThreads<P, kRegR>, kLowRegs<P, kRegR> ? 5 
     }
 
     if (a.stats != nullptr && lane == 0) {
-        atomicAdd(a.stats + kStatQueries, c_q);
-        atomicAdd(a.stats + kStatExpansions, c_exp);
-        atomicAdd(a.stats + kStatDist0, c_d0);
-        atomicAdd(a.stats + kStatDistUpper, c_du);
-        atomicAdd(a.stats + kStatLinkBytes, c_lb);
-        atomicAdd(a.stats + kStatRowBytes, c_rb);
-        atomicAdd(a.stats + kStatRerankBytes, c_rr);
-        atomicAdd(a.stats + kStatDuplicates, c_dup);
-        atomicAdd(a.stats + kStatPrefetchHits, c_pf);
-        atomicAdd(a.stats + kStatLearnedStops, c_stop);
+        using u64 = unsigned long long;
+        atomicAdd(a.stats + kStatQueries, static_cast<u64>(c_q));
+        atomicAdd(a.stats + kStatExpansions, static_cast<u64>(c_exp));
+        atomicAdd(a.stats + kStatDist0, static_cast<u64>(c_d0));
+        atomicAdd(a.stats + kStatDistUpper, static_cast<u64>(c_du));
+        atomicAdd(a.stats + kStatLinkBytes, 4ull * c_lw);
+        atomicAdd(a.stats + kStatRowBytes, (static_cast<u64>(c_d0) + c_du) * g.row_bytes);
+        atomicAdd(a.stats + kStatRerankBytes, static_cast<u64>(c_rr) * (g.row32 * 4));
+        atomicAdd(a.stats + kStatDuplicates, static_cast<u64>(c_dup));
+        atomicAdd(a.stats + kStatPrefetchHits, static_cast<u64>(c_pf));
+        atomicAdd(a.stats + kStatLearnedStops, static_cast<u64>(c_stop));
     }
 }
 
