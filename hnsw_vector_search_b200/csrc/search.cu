@@ -31,6 +31,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <mutex>
@@ -226,9 +227,12 @@ __device__ __forceinline__ float row_distance(const float* q, const unsigned cha
 // them is on, so plain searches carry neither their code nor their registers; BF16 ef 36 7 %
 // faster). Without that code the compiler's own register target for the shared-memory-beam
 // kernels fell to 80 with spills, so those are bounded like the rest at 128 (2 blocks of 256).
-template <int P, bool kL2, bool kRegR, bool kLearn>
+// kPass: the pass compiled (0 the whole search, 1 the descent of an ordered launch, 2 its layer-0
+// pass), so each kernel carries only the code its pass runs.
+template <int P, bool kL2, bool kRegR, bool kLearn, int kPass>
 __global__ void __launch_bounds__(kMaxThreads<P, kRegR>, kLowRegs<P, kRegR> ? 5 : (kLearn ? 0 : 2))
     search_kernel(const SearchArgs a) {
+    constexpr std::uint32_t pass = kPass;
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = static_cast<int>(threadIdx.x & 31);
     const int warp = static_cast<int>(threadIdx.x >> 5);
@@ -280,18 +284,18 @@ __global__ void __launch_bounds__(kMaxThreads<P, kRegR>, kLowRegs<P, kRegR> ? 5 
     for (;;) {
         std::uint32_t qi = 0;
         if (lane == 0) {
-            qi = atomicAdd(a.pass == 2 ? a.claim + 1 : a.claim, 1u);
+            qi = atomicAdd(pass == 2 ? a.claim + 1 : a.claim, 1u);
         }
         qi = __shfl_sync(kFull, qi, 0);
         if (qi >= nq) {
             break;
         }
-        if (a.pass == 2) {
+        if (pass == 2) {
             qi = a.order[qi];
             if (a.entry_ids[qi] == kNoId) {
                 continue;  // failed its checks in the descent pass, which wrote its row
             }
-        } else if (a.pass == 1 && lane == 0) {
+        } else if (pass == 1 && lane == 0) {
             a.entry_ids[qi] = kNoId;  // until the descent below completes
         }
         const std::uint32_t k = a.k_per_q != nullptr ? a.k_per_q[qi] : a.k;
@@ -350,12 +354,12 @@ __global__ void __launch_bounds__(kMaxThreads<P, kRegR>, kLowRegs<P, kRegR> ? 5 
             }
             __syncwarp();
         }
-        if (a.pass != 2) {
+        if (pass != 2) {
             ++c_q;
         }
         float qlen = 0.0F;
         float proj[4] = {0.0F, 0.0F, 0.0F, 0.0F};
-        if ((learned || tracing) && a.pass != 1) {
+        if ((learned || tracing) && pass != 1) {
             qlen = sqrtf(warp_raw<kFP32, false>(q, reinterpret_cast<const unsigned char*>(q), g.dim,
                                                 g.row32 * 4, lane));
             const float inv = 1.0F / fmaxf(qlen, 1e-20F);
@@ -372,7 +376,7 @@ __global__ void __launch_bounds__(kMaxThreads<P, kRegR>, kLowRegs<P, kRegR> ? 5 
         // descent pass's result).
         std::uint32_t cur = g.entry;
         float curd = 0.0F;
-        if (a.pass == 2) {
+        if (pass == 2) {
             cur = a.entry_ids[qi];
             curd = a.entry_d[qi];
         } else {
@@ -452,7 +456,7 @@ __global__ void __launch_bounds__(kMaxThreads<P, kRegR>, kLowRegs<P, kRegR> ? 5 
                     }
                 }
             }
-            if (a.pass == 1) {
+            if (pass == 1) {
                 __syncwarp();
                 if (lane == 0) {
                     a.entry_d[qi] = curd;
@@ -902,11 +906,18 @@ cudaError_t resident_blocks(const void* kernel, int device, int threads, std::si
     return cudaSuccess;
 }
 
+// The kernel of pass `kPass` for these arguments (the learned-stop variant when the stop or
+// tracing is on).
+template <int P, bool kL2, bool kRegR, int kPass>
+const void* pass_kernel(const SearchArgs& args) {
+    const bool learn = args.stop_enabled != nullptr || args.trace.truth != nullptr;
+    return learn ? reinterpret_cast<const void*>(&search_kernel<P, kL2, kRegR, true, kPass>)
+                 : reinterpret_cast<const void*>(&search_kernel<P, kL2, kRegR, false, kPass>);
+}
+
 template <int P, bool kL2, bool kRegR>
 cudaError_t launch_typed(SearchArgs& args, const SearchPlan& plan, std::size_t smem,
                          cudaStream_t stream) {
-    const bool learn = args.stop_enabled != nullptr || args.trace.truth != nullptr;
-    auto* kernel = learn ? &search_kernel<P, kL2, kRegR, true> : &search_kernel<P, kL2, kRegR, false>;
     if (plan.warps_per_block < 1 || plan.warps_per_block * 32 > kMaxThreads<P, kRegR>) {
         return cudaErrorInvalidValue;  // a plan beyond max_warps_per_block
     }
@@ -915,41 +926,71 @@ cudaError_t launch_typed(SearchArgs& args, const SearchPlan& plan, std::size_t s
     if (err != cudaSuccess) {
         return err;
     }
-    err = raise_smem_limit(reinterpret_cast<const void*>(kernel), device, smem);
-    if (err != cudaSuccess) {
-        return err;
-    }
     const int threads = plan.warps_per_block * 32;
-    int blocks = plan.blocks;
-    if (blocks <= 0) {
-        err = resident_blocks(reinterpret_cast<const void*>(kernel), device, threads, smem, blocks);
-        if (err != cudaSuccess) {
-            return err;
-        }
-    }
     const std::uint32_t nq = args.nq;
     const std::uint32_t needed = (nq + plan.warps_per_block - 1) / plan.warps_per_block;
-    if (args.nq_device == nullptr && static_cast<std::uint32_t>(blocks) > needed) {
-        blocks = static_cast<int>(needed > 0 ? needed : 1);
-    }
-    if (plan.global_slots > 0) {
-        // One table per warp of the grid: the caller's buffer must hold them all.
-        if (args.gvisited == nullptr || args.gepoch == nullptr || args.gslots != plan.global_slots ||
-            args.gstride < args.gslots ||
-            static_cast<std::uint64_t>(blocks) * plan.warps_per_block > args.gwarps) {
-            return cudaErrorInvalidValue;
+    // Sets the kernel's shared-memory limit and finds its grid: as many blocks as reside (or the
+    // plan's count), trimmed to the batch unless the batch size is read on the device.
+    const auto prepare = [&](const void* kernel, int& blocks) -> cudaError_t {
+        cudaError_t e = raise_smem_limit(kernel, device, smem);
+        if (e != cudaSuccess) {
+            return e;
         }
-    } else {
-        args.gvisited = nullptr;
-    }
+        blocks = plan.blocks;
+        if (blocks <= 0) {
+            e = resident_blocks(kernel, device, threads, smem, blocks);
+            if (e != cudaSuccess) {
+                return e;
+            }
+        }
+        if (args.nq_device == nullptr && static_cast<std::uint32_t>(blocks) > needed) {
+            blocks = static_cast<int>(needed > 0 ? needed : 1);
+        }
+        return cudaSuccess;
+    };
+    // One global visited table per warp of the layer-0 grid: the caller's buffer must hold them.
+    const auto check_tables = [&](int blocks) -> cudaError_t {
+        if (plan.global_slots > 0) {
+            if (args.gvisited == nullptr || args.gepoch == nullptr ||
+                args.gslots != plan.global_slots || args.gstride < args.gslots ||
+                static_cast<std::uint64_t>(blocks) * plan.warps_per_block > args.gwarps) {
+                return cudaErrorInvalidValue;
+            }
+        } else {
+            args.gvisited = nullptr;
+        }
+        return cudaSuccess;
+    };
+    using Kernel = void (*)(SearchArgs);
     if (args.entry_ids == nullptr || args.entry_d == nullptr || args.order == nullptr) {
+        const void* k0 = pass_kernel<P, kL2, kRegR, 0>(args);
+        int blocks = 0;
+        if (err = prepare(k0, blocks); err != cudaSuccess) {
+            return err;
+        }
+        if (err = check_tables(blocks); err != cudaSuccess) {
+            return err;
+        }
         args.pass = 0;
-        kernel<<<blocks, threads, smem, stream>>>(args);
+        reinterpret_cast<Kernel>(const_cast<void*>(k0))<<<blocks, threads, smem, stream>>>(args);
         g_last_kernels = 1;
         return cudaGetLastError();
     }
+    const void* k1 = pass_kernel<P, kL2, kRegR, 1>(args);
+    const void* k2 = pass_kernel<P, kL2, kRegR, 2>(args);
+    int blocks1 = 0;
+    int blocks2 = 0;
+    if (err = prepare(k1, blocks1); err != cudaSuccess) {
+        return err;
+    }
+    if (err = prepare(k2, blocks2); err != cudaSuccess) {
+        return err;
+    }
+    if (err = check_tables(blocks2); err != cudaSuccess) {
+        return err;
+    }
     args.pass = 1;
-    kernel<<<blocks, threads, smem, stream>>>(args);
+    reinterpret_cast<Kernel>(const_cast<void*>(k1))<<<blocks1, threads, smem, stream>>>(args);
     if (err = cudaGetLastError(); err != cudaSuccess) {
         return err;
     }
@@ -958,7 +999,7 @@ cudaError_t launch_typed(SearchArgs& args, const SearchPlan& plan, std::size_t s
         return err;
     }
     args.pass = 2;
-    kernel<<<blocks, threads, smem, stream>>>(args);
+    reinterpret_cast<Kernel>(const_cast<void*>(k2))<<<blocks2, threads, smem, stream>>>(args);
     g_last_kernels = 3;
     return cudaGetLastError();
 }
@@ -1094,31 +1135,26 @@ std::uint32_t search_warps(SearchArgs& args, const SearchPlan& plan) {
         return blocks;
     };
     const bool l2 = args.g.metric == 0;
-    // The kernel launch_search will pick (the register-beam variants for small capacities, the
-    // learned-stop variants when the stop or tracing is on).
+    // The kernels that read global tables (the whole-search and layer-0 passes) as launch_search
+    // will pick them (register-beam variants for small capacities, learned-stop variants when the
+    // stop or tracing is on); the tables must cover the larger of their grids.
     const bool reg = plan.efcap <= kRegBeamCap;
-    const bool learn = args.stop_enabled != nullptr || args.trace.truth != nullptr;
-    const auto pick = [&](auto p_tag) -> const void* {
+    const auto pick = [&](auto p_tag, auto pass_tag) -> const void* {
         constexpr int P = decltype(p_tag)::value;
+        constexpr int kPass = decltype(pass_tag)::value;
         if (reg) {
-            if (learn) {
-                return l2 ? reinterpret_cast<const void*>(&search_kernel<P, true, true, true>)
-                          : reinterpret_cast<const void*>(&search_kernel<P, false, true, true>);
-            }
-            return l2 ? reinterpret_cast<const void*>(&search_kernel<P, true, true, false>)
-                      : reinterpret_cast<const void*>(&search_kernel<P, false, true, false>);
+            return l2 ? pass_kernel<P, true, true, kPass>(args) : pass_kernel<P, false, true, kPass>(args);
         }
-        if (learn) {
-            return l2 ? reinterpret_cast<const void*>(&search_kernel<P, true, false, true>)
-                      : reinterpret_cast<const void*>(&search_kernel<P, false, false, true>);
-        }
-        return l2 ? reinterpret_cast<const void*>(&search_kernel<P, true, false, false>)
-                  : reinterpret_cast<const void*>(&search_kernel<P, false, false, false>);
+        return l2 ? pass_kernel<P, true, false, kPass>(args) : pass_kernel<P, false, false, kPass>(args);
     };
-    const void* kernel = args.g.precision == 0   ? pick(std::integral_constant<int, kFP32>{})
-                         : args.g.precision == 1 ? pick(std::integral_constant<int, kBF16>{})
-                                                 : pick(std::integral_constant<int, kFP8>{});
-    return static_cast<std::uint32_t>(grid_of(kernel) * plan.warps_per_block);
+    const auto pick_pass = [&](auto pass_tag) -> const void* {
+        return args.g.precision == 0   ? pick(std::integral_constant<int, kFP32>{}, pass_tag)
+               : args.g.precision == 1 ? pick(std::integral_constant<int, kBF16>{}, pass_tag)
+                                       : pick(std::integral_constant<int, kFP8>{}, pass_tag);
+    };
+    const int grid = std::max(grid_of(pick_pass(std::integral_constant<int, 0>{})),
+                              grid_of(pick_pass(std::integral_constant<int, 2>{})));
+    return static_cast<std::uint32_t>(grid * plan.warps_per_block);
 }
 
 std::size_t global_visited_bytes(std::uint32_t stride, std::uint32_t warps) {
