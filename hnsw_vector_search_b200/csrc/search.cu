@@ -15,16 +15,20 @@
 //      has no unexpanded entry left).
 //   4. write the first min(k, |R|) entries, closest first (ties by smaller id).
 //
-// Memory traffic, the bound of this kernel: each expansion reads one link block (one 128-byte line
-// at M = 16) and gathers the unvisited neighbors' rows with 16-byte cp.async copies into shared
-// memory, all rows of a round in flight together; the link block of the next likely expansion
-// (the second-best unexpanded entry) is prefetched while the current one is processed.
+// Memory traffic: each expansion reads one link block (one 128-byte line at M = 16) and gathers
+// the unvisited neighbors' rows with 16-byte cp.async copies into shared memory, all rows of a
+// round in flight together; the link block of the next expansion, predicted exactly before the
+// merge (the closer of R's first unexpanded entry and the round's best admissible candidate), is
+// prefetched while the merge runs. The kernel is bound by the latency of that dependent chain
+// per expansion and by instruction issue, not by DRAM bandwidth; the rest of this file keeps the
+// chain short (register result list, bucketed filter, ballot merge, unrolled d = 128 distances)
+// and the registers few (one kernel per pass and per learned-stop use).
 //
 // The visited set is a per-warp shared-memory open-addressing hash of 4-slot buckets (one 16-byte
-// load per bucket, first_visit_bucket). It never reports an
-// unvisited node as visited. If its probe limit is reached it reports "unvisited" and the node is
-// scored again; the merge then drops the copy already in R (equal distance and id), so results
-// stay exact and the only cost is the extra row read (counted in kStatDuplicates).
+// load per bucket, first_visit_bucket). It never reports an unvisited node as visited. If its
+// probe limit is reached it reports "unvisited" and the node is scored again; the merge then drops
+// the copy already in R (equal distance and id), so results stay exact and the only cost is the
+// extra row read (counted in kStatDuplicates).
 //
 // Every loop is bounded (the walk cannot run longer than the node count), and no kernel waits on
 // another thread or block: cp.async completion is a hardware wait.
