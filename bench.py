@@ -40,6 +40,10 @@ N_QUERIES = 10_000
 K = 10
 M, EF_CONSTRUCTION, SEED = 16, 200, 42
 EF_SWEEP = [16, 20, 24, 28, 32, 36, 40, 44, 48, 56, 64, 80, 96, 128, 192, 256, 384, 512]
+# ef values of the id-parity comparison with the reference (the config-2 sweep, 16..512).
+PARITY_EFS = [16, 24, 32, 48, 64, 96, 128, 192, 256, 384, 512]
+PARITY_MIN_IDS = 0.999    # share of queries whose k ids equal the reference's, at every ef
+PARITY_MAX_DRECALL = 0.002
 TRAIN_QUERIES, CAL_QUERIES = 20_000, 5_000
 TARGET_RECALL = 0.95
 METRIC = "QPS at recall@10>=0.95, 1Mx128 L2, 1xB200: learned/BF16 vs plain GPU HNSW"
@@ -195,19 +199,15 @@ def run_reference(args, rank, world):
     import oracle as o
     ref = o.RefHnsw.load(graph)
     threads = os.cpu_count() or 1
-    sample = queries[:2000]
-    truth_file = CACHE / "sift_like_1m_truth_ref2000.npy"
-    if truth_file.exists():
-        truth = np.load(truth_file)
-    else:  # the reference's own exact search judges the reference's recall
-        bf = o.RefBruteForce(base.shape[1], 0)
-        bf.add(base)
-        truth, _, _ = bf.search_batch(sample, K, threads)
-        np.save(truth_file, truth)
+    sample = queries  # the same 10,000 queries the GPU arm searches and judges
+    truth = reference_truth(base, sample, threads)
     chosen = EF_SWEEP[-1]
+    sweep = []
     for ef in EF_SWEEP:
         ids, _, _ = ref.search_batch(sample, K, ef, threads)
-        if recall_at_10(ids, truth) >= TARGET_RECALL:
+        rec = recall_at_10(ids, truth)
+        sweep.append({"ef": ef, "recall": round(rec, 4)})
+        if rec >= TARGET_RECALL:
             chosen = ef
             break
     ids, _, _ = ref.search_batch(sample, K, chosen, threads)
@@ -222,12 +222,34 @@ def run_reference(args, rank, world):
             "ms_per_step": 1000 * total / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": "1M x 128 L2 sift-like, 10k queries, M16 efc200, k10",
-                       "ef": chosen, "recall_at_10": rec, "step": f"{len(sample)} queries"},
+                       "ef": chosen, "recall_at_10": round(rec, 4),
+                       "step": f"{len(sample)} queries (the GPU arm's batch)",
+                       "judge": "the reference's BruteForceIndex on the same 10,000 queries"},
+            "sweep": sweep,
             "cpu_baseline": {"value": value, "unit": "queries/s", "cores": threads,
                              "kind": "reference", "sample": f"{len(sample)} queries per step"},
             "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def reference_truth(base, queries, threads):
+    """Exact top-10 ids of `queries` by the reference's own BruteForceIndex (all host cores);
+    cached. Judges the reference arm's recall on the queries the GPU arm searches."""
+    f = CACHE / "sift_like_1m_truth_ref.npy"
+    if f.exists():
+        t = np.load(f)
+        if t.shape == (len(queries), K):
+            return t
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as o
+    t0 = time.time()
+    bf = o.RefBruteForce(base.shape[1], 0)
+    bf.add(base)
+    truth, _, _ = bf.search_batch(queries, K, threads)
+    np.save(f, truth)
+    log(f"reference brute force of {len(queries)} queries: {time.time() - t0:.1f} s")
+    return truth
 
 
 def ground_truth(base, queries):
@@ -389,38 +411,56 @@ def main():
     eligible = [n for n in results if results[n]["recall"] >= TARGET_RECALL] or list(results)
     best = max(eligible, key=lambda n: results[n]["qps"])
     r = results[best]
-    st = r["stats"]
-    algorithmic = st[4] + st[5] + st[6] + nq * 128 * 4  # links + rows + rerank rows + queries
-    per_launch_s = r["seconds"] / args.steps
-    achieved = algorithmic / per_launch_s / 1e9
     peak, peak_kind = peaks()
-    traffic = ncu_traffic(f"search_{best}")
+    # Roofline of every mode, two readings: algorithmic bytes (the kernel's own counters: links,
+    # traversal rows, re-rank rows, queries) and DRAM bytes (ncu's dram__bytes of the same call,
+    # profiles/roofline_traffic.txt; rows served from L2 count in the first, not the second).
+    roofline_by_mode = {}
+    for name, x in results.items():
+        st = x["stats"]
+        algorithmic = st[4] + st[5] + st[6] + nq * 128 * 4
+        per_launch_s = x["seconds"] / args.steps
+        achieved = algorithmic / per_launch_s / 1e9
+        traffic = ncu_traffic(f"search_{name}@ef{x['ef']}")
+        roofline_by_mode[name] = {
+            "ef": x["ef"], "algorithmic_bytes_per_launch": int(algorithmic),
+            "us_per_launch": per_launch_s * 1e6, "achieved": achieved, "frac": achieved / peak,
+            "traffic": traffic,
+            "achieved_dram": None if traffic is None else traffic / per_launch_s / 1e9,
+            "frac_dram": None if traffic is None else traffic / per_launch_s / 1e9 / peak}
+    rb = roofline_by_mode[best]
 
-    # End to end through the public host API: page-locked host queries in, results out into
-    # page-locked host arrays, per step (the kernel reads the queries and writes the results
+    # End to end through the public host API, per mode: page-locked host queries in, results out
+    # into page-locked host arrays, per step (the kernel reads the queries and writes the results
     # across the bus in place; every byte still moves each step).
     h_q = torch.from_numpy(queries).pin_memory().numpy()
-    ef_best = r["ef"]
-    opts = dict(modes)[best]
     h_out = (torch.empty((nq, K), dtype=torch.int32).pin_memory().numpy().view(np.uint32),
              torch.empty((nq, K), dtype=torch.float32).pin_memory().numpy(),
              torch.empty(nq, dtype=torch.int32).pin_memory().numpy().view(np.uint32))
-    want = ix.search_batch(h_q, K, ef_best, device=local, **opts)
-    if pg is not None:
-        pg.barrier()
-    e2e_total = 0.0
-    for _ in range(args.steps):
-        h_out[0].fill(0)
-        t0 = time.perf_counter()
-        ix.search_batch(h_q, K, ef_best, device=local, out=h_out, **opts)
-        e2e_total += time.perf_counter() - t0
-        if not np.array_equal(h_out[0], want[0]):
-            raise RuntimeError("end-to-end results differ from the reference call's")
-    if pg is not None:
-        t = torch.tensor([e2e_total], device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e_total = float(t.item())
+    e2e_by_mode = {}
+    e2e_kernels = 0
+    for name, opts in modes:
+        ef_m = results[name]["ef"]
+        want = ix.search_batch(h_q, K, ef_m, device=local, **opts)
+        if pg is not None:
+            pg.barrier()
+        e2e_total = 0.0
+        for _ in range(args.steps):
+            h_out[0].fill(0)
+            t0 = time.perf_counter()
+            ix.search_batch(h_q, K, ef_m, device=local, out=h_out, **opts)
+            e2e_total += time.perf_counter() - t0
+            if not np.array_equal(h_out[0], want[0]):
+                raise RuntimeError("end-to-end results differ from the reference call's")
+        if pg is not None:
+            t = torch.tensor([e2e_total], device=dev)
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            e2e_total = float(t.item())
+        e2e_by_mode[name] = {"qps": nq * world * args.steps / e2e_total, "ef": ef_m}
+        if name == best:
+            e2e_kernels = int(v.lib().vdx_search_kernels_last())  # one end-to-end call's launches
 
+    parity = parity_section(v, ix, graph, queries, truth, local, learned_info) if rank == 0 else None
     brute = bruteforce_section(v, torch, base, queries, dev) if rank == 0 else None
     if rank == 0:
         cpu = cpu_baseline(graph, queries, results["fp32"]["ef"])
@@ -428,7 +468,6 @@ def main():
         pg.barrier()
     if rank == 0:
         kernels_per_step = kernels_by_mode[best]  # one timed device step's launches
-        e2e_kernels = int(v.lib().vdx_search_kernels_last())  # one end-to-end call's launches
         line = {
             "metric": METRIC, "value": r["qps"], "unit": "queries/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
@@ -444,21 +483,26 @@ def main():
                            "recall_at_10": round(results["fp32"]["recall"], 4)},
             "speedup_vs_plain_fp32": r["qps"] / results["fp32"]["qps"],
             "learned": learned_info,
-            "modes": {n: {"qps": x["qps"], "ef": x["ef"], "recall_at_10": round(x["recall"], 4)}
+            "modes": {n: {"qps": x["qps"], "ef": x["ef"], "recall_at_10": round(x["recall"], 4),
+                          "speedup_vs_plain_fp32": x["qps"] / results["fp32"]["qps"]}
                       for n, x in results.items()},
             "sweep": sweep,
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+            "parity": parity,
+            "roofline": {"bound": "hbm", "achieved": rb["achieved"], "peak": peak, "unit": "GB/s",
+                         "frac": rb["frac"], "traffic": rb["traffic"], "frac_dram": rb["frac_dram"],
+                         "peak_kind": peak_kind,
                          "kernel": f"one ordered search call ({best}): search_kernel descent pass, "
                                    "order_kernel, search_kernel layer-0 pass; CUDA-event time of "
                                    "the call, traffic of both passes",
-                         "algorithmic_bytes_per_launch": algorithmic},
+                         "algorithmic_bytes_per_launch": rb["algorithmic_bytes_per_launch"]},
+            "roofline_by_mode": roofline_by_mode,
             "cpu_baseline": cpu,
-            "e2e": {"value": nq * world * args.steps / e2e_total, "unit": "queries/s",
+            "e2e": {"value": e2e_by_mode[best]["qps"], "unit": "queries/s",
                     "h2d_bytes_per_step": int(queries.nbytes),
                     "d2h_bytes_per_step": int(nq * K * 8 + nq * 4),
                     "api": "HnswIndex.search_batch(page-locked queries, out=page-locked arrays)",
                     "gpu_launches_per_call": e2e_kernels},
+            "e2e_by_mode": e2e_by_mode,
             "gpu_launches": args.steps * kernels_per_step,
             "clocks": clock_summary,
             "bruteforce": brute,
@@ -467,6 +511,57 @@ def main():
     if pg is not None:
         pg.barrier()
         pg.destroy_process_group()
+
+
+def parity_section(v, ix, graph, queries, truth, device, learned_info) -> dict:
+    """Id parity with the reference on the headline graph: for every ef of PARITY_EFS the
+    reference's own HnswIndex::search_batch (src/hnsw.cpp:490-501, all host cores) and this
+    library's FP32 and BF16 (+ FP32 re-rank of 40) searches run on all 10,000 test queries of the
+    same loaded file. Per ef and mode: the share of queries whose k ids (in order) and count equal
+    the reference's, the share whose distance bits also do, both recalls against exact brute
+    force and their difference. `pass` holds the bar: ids identical on >= 99.9 % of queries and
+    |recall difference| <= 0.002 at every ef. The learned stop changes where the beam stops by
+    design, so for it only recall is compared, at its ef cap."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as o
+    ref = o.RefHnsw.load(graph)
+    threads = os.cpu_count() or 1
+    table = {"fp32": [], "bf16": []}
+    ref_seconds = 0.0
+    ref_recall = {}
+    for ef in PARITY_EFS:
+        t0 = time.perf_counter()
+        rid, rd, rc = ref.search_batch(queries, K, ef, threads)
+        ref_seconds += time.perf_counter() - t0
+        rrec = recall_at_10(rid, truth)
+        ref_recall[ef] = rrec
+        for name, opts in (("fp32", {}), ("bf16", {"precision": "bf16", "rerank": 40})):
+            gid, gd, gc = ix.search_batch(queries, K, ef, device=device, **opts)
+            same = np.all(gid == rid, axis=1) & (gc == rc)
+            bits = same & np.all(gd.view(np.uint32) == rd.view(np.uint32), axis=1)
+            grec = recall_at_10(gid, truth)
+            table[name].append({"ef": ef, "ids_identical_frac": float(same.mean()),
+                                "dist_bits_identical_frac": float(bits.mean()),
+                                "recall": round(grec, 4), "reference_recall": round(rrec, 4),
+                                "delta_recall": round(grec - rrec, 5)})
+    summary = {}
+    for name, rows in table.items():
+        worst_ids = min(x["ids_identical_frac"] for x in rows)
+        worst_dr = max(abs(x["delta_recall"]) for x in rows)
+        summary[name] = {"min_ids_identical_frac": worst_ids, "max_abs_delta_recall": worst_dr,
+                         "pass": bool(worst_ids >= PARITY_MIN_IDS and worst_dr <= PARITY_MAX_DRECALL)}
+    out = {"queries": len(queries), "k": K, "efs": PARITY_EFS, "reference_threads": threads,
+           "reference_seconds": round(ref_seconds, 2),
+           "bar": {"min_ids_identical_frac": PARITY_MIN_IDS, "max_abs_delta_recall": PARITY_MAX_DRECALL},
+           "summary": summary, "by_ef": table}
+    cap = learned_info.get("ef_cap")
+    if cap:
+        rid, _, _ = ref.search_batch(queries, K, cap, threads)
+        gid, _, _ = ix.search_batch(queries, K, cap, device=device, precision="bf16", rerank=40,
+                                    learned_stop=True, stop_threshold=learned_info["threshold"])
+        out["learned_bf16"] = {"ef_cap": cap, "recall": round(recall_at_10(gid, truth), 4),
+                               "reference_recall_at_cap": round(recall_at_10(rid, truth), 4)}
+    return out
 
 
 def learned_mode(v, ix, base, graph, device) -> dict:

@@ -116,6 +116,14 @@ def lib() -> ctypes.CDLL:
     return L
 
 
+class DeviceTimeout(RuntimeError):
+    """VDX_ERR_DEVICE_TIMEOUT: a bounded device wait gave up; the kernel released what it held."""
+
+
+class DeviceBounds(RuntimeError):
+    """VDX_ERR_DEVICE_BOUNDS: a kernel met an out-of-range link id in the device graph."""
+
+
 def _raise(status: int) -> None:
     if status == 0:
         return
@@ -126,6 +134,10 @@ def _raise(status: int) -> None:
         raise OverflowError(msg)
     if status == 3:
         raise OSError(msg)
+    if status == 6:
+        raise DeviceTimeout(msg)
+    if status == 7:
+        raise DeviceBounds(msg)
     raise RuntimeError(msg)
 
 

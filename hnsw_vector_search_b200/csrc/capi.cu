@@ -37,6 +37,12 @@ vdx_status guarded(Fn&& fn) {
     } catch (const vdx::gpu::CudaError& e) {
         g_error = e.what();
         return VDX_ERR_CUDA;
+    } catch (const vdx::gpu::DeviceTimeout& e) {
+        g_error = e.what();
+        return VDX_ERR_DEVICE_TIMEOUT;
+    } catch (const vdx::gpu::DeviceBounds& e) {
+        g_error = e.what();
+        return VDX_ERR_DEVICE_BOUNDS;
     } catch (const std::runtime_error& e) {
         g_error = e.what();
         return VDX_ERR_IO;
@@ -283,6 +289,15 @@ vdx_status vdx_search_batch_device(const vdx_index* index, const float* d_querie
         const vdx::SearchOptions o = options_of(opts);
         vdx::detail::check_query_shape("HnswIndex::search_batch", {h.metric(), h.dim(), h.size()},
                                        dim, d_k == nullptr ? k_uniform : 1);
+        if (nq > 0) {
+            require(d_queries, "d_queries");
+            require(d_ids, "d_ids");
+            require(d_dists, "d_dists");
+            require(d_counts, "d_counts");
+            if (d_k == nullptr && out_stride < k_uniform) {
+                throw std::invalid_argument("vdx_search_batch_device: out_stride is smaller than k");
+            }
+        }
         auto s = static_cast<cudaStream_t>(stream);
         vdx::gpu::use_device(o.device);
         vdx::gpu::check(cudaMemsetAsync(d_work, 0, vdx_work_words() * 4, s), "reset work words");
@@ -293,7 +308,6 @@ vdx_status vdx_search_batch_device(const vdx_index* index, const float* d_querie
             }
             return;
         }
-        require(d_queries, "d_queries");
         const vdx::DeviceGraph& g = h.device_graph(o.device, o.precision);
         vdx::dev::SearchArgs a;
         a.g = g.view;

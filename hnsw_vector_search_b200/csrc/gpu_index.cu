@@ -238,11 +238,11 @@ void raise_status(std::uint32_t code, const char* where) {
             throw std::invalid_argument(
                 std::format("{}: the cosine metric can't normalize a zero query", where));
         case dev::kErrBounds:
-            throw std::runtime_error(std::format("{}: the device graph holds an out-of-range link", where));
+            throw DeviceBounds(std::format("{}: the device graph holds an out-of-range link", where));
         case dev::kErrCapacity:
             throw std::invalid_argument(std::format("{}: ef exceeds the GPU search capacity", where));
         case dev::kErrTimeout:
-            throw CudaError(std::format("{}: a device wait timed out", where));
+            throw DeviceTimeout(std::format("{}: a device wait timed out", where));
         default:
             throw std::runtime_error(std::format("{}: device error {}", where, code));
     }

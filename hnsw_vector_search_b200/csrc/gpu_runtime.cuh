@@ -16,6 +16,16 @@ struct CudaError : std::runtime_error {
     explicit CudaError(const std::string& what) : std::runtime_error(what) {}
 };
 
+// A bounded device wait that gave up; the kernel released what it held (VDX_ERR_DEVICE_TIMEOUT).
+struct DeviceTimeout : std::runtime_error {
+    explicit DeviceTimeout(const std::string& what) : std::runtime_error(what) {}
+};
+
+// An out-of-range link id met in the device graph (VDX_ERR_DEVICE_BOUNDS).
+struct DeviceBounds : std::runtime_error {
+    explicit DeviceBounds(const std::string& what) : std::runtime_error(what) {}
+};
+
 // One host thread's buffers on one device: its stream, query and result buffers (grown on
 // demand), 256 bytes of status / counter / statistics words and their pinned host copy.
 // Layout of `small` (u32 words): [0] error code, [1] first failing row, [2] work counter,

@@ -18,7 +18,13 @@
 //
 // Set-up: the first call on each device looks up the array's device address with
 // cudaGetSymbolAddress (in host code the array's name is only a host-side stand-in, not a device
-// address) and keeps it; make that first call before any stream capture begins.
+// address) and keeps it; make that first call before any stream capture begins. The address is
+// kept for the life of the process: a cudaDeviceReset (or any teardown of the primary context)
+// after that first call is not supported, since the kept address would then be stale.
+//
+// The learned stop is not offered here: its network lives in device memory that the index
+// allocates on first use, so a call asking for it is rejected (VDX_ERR_INVALID_ARGUMENT)
+// rather than silently running the plain search.
 
 #include <cuda_runtime.h>
 
@@ -74,6 +80,11 @@ extern "C" vdx_status vdx_search_batch_device_noalloc(
             if (opts->precision > 2) {
                 throw std::invalid_argument("unknown precision");
             }
+            if (opts->learned_stop != 0) {
+                throw std::invalid_argument(
+                    "vdx_search_batch_device_noalloc: the learned stop is not available without "
+                    "allocation; use vdx_search_batch_device");
+            }
             o.precision = static_cast<vdx::Precision>(opts->precision);
             o.rerank = opts->rerank;
             o.device = opts->device;
@@ -81,6 +92,22 @@ extern "C" vdx_status vdx_search_batch_device_noalloc(
         const char* where = "HnswIndex::search_batch";
         vdx::detail::check_query_shape(where, {h.metric(), h.dim(), h.size()}, dim,
                                        d_k == nullptr ? k_uniform : 1);
+        if (nq > 0) {
+            const auto require = [](const void* p, const char* what) {
+                if (p == nullptr) {
+                    throw std::invalid_argument(std::string("vdx_search_batch_device_noalloc: ") +
+                                                what + " is NULL");
+                }
+            };
+            require(d_queries, "d_queries");
+            require(d_ids, "d_ids");
+            require(d_dists, "d_dists");
+            require(d_counts, "d_counts");
+            if (d_k == nullptr && out_stride < k_uniform) {
+                throw std::invalid_argument(
+                    "vdx_search_batch_device_noalloc: out_stride is smaller than k");
+            }
+        }
         if (vdx_work_words() > kStaticWorkWords) {
             throw std::length_error(
                 "vdx_search_batch_device_noalloc: the launch needs " +
@@ -142,6 +169,12 @@ extern "C" vdx_status vdx_search_batch_device_noalloc(
     } catch (const vdx::gpu::CudaError& e) {
         vdx::capi::set_last_error(e.what());
         return VDX_ERR_CUDA;
+    } catch (const vdx::gpu::DeviceTimeout& e) {
+        vdx::capi::set_last_error(e.what());
+        return VDX_ERR_DEVICE_TIMEOUT;
+    } catch (const vdx::gpu::DeviceBounds& e) {
+        vdx::capi::set_last_error(e.what());
+        return VDX_ERR_DEVICE_BOUNDS;
     } catch (const std::exception& e) {
         vdx::capi::set_last_error(e.what());
         return VDX_ERR_INTERNAL;

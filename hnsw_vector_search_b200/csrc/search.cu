@@ -739,8 +739,9 @@ __global__ void __launch_bounds__(kMaxThreads<P, kRegR>, kLowRegs<P, kRegR> ? 5 
             r = rr;
         }
 
-        // 4. Results.
-        const int cnt = min(r, static_cast<int>(k));
+        // 4. Results (a per-query k beyond the row width is cut to the width, so the count
+        // never names entries that were not written).
+        const int cnt = min(min(r, static_cast<int>(k)), static_cast<int>(a.out_stride));
         for (std::uint32_t i = lane; i < a.out_stride; i += 32) {
             if (static_cast<int>(i) < cnt) {
                 oid[i] = rid[i] & kIdMask;

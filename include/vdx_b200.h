@@ -30,7 +30,15 @@ typedef enum vdx_status {
     VDX_ERR_LENGTH = 2,           /* std::length_error */
     VDX_ERR_IO = 3,               /* std::runtime_error from save / load */
     VDX_ERR_CUDA = 4,             /* a CUDA call failed, or no device is present */
-    VDX_ERR_INTERNAL = 5
+    VDX_ERR_INTERNAL = 5,
+    /* No reference counterpart (the reference has no device code). A bounded device wait gave up
+     * (the tensor-core brute force's pipeline barriers): the kernel drained its own copies and
+     * tensor-core work, freed its tensor memory and returned, so the context stays usable and
+     * the next call may be retried. */
+    VDX_ERR_DEVICE_TIMEOUT = 6,
+    /* No reference counterpart. A kernel met a link id outside the index in the device copy of
+     * the graph (a corrupted device mirror); the access was skipped. */
+    VDX_ERR_DEVICE_BOUNDS = 7
 } vdx_status;
 
 /* Metric codes are the file format's (docs/FORMAT.md "Header"): 0 L2, 1 inner product, 2 cosine. */
@@ -139,7 +147,10 @@ VDX_API vdx_status vdx_index_upload(const vdx_index* index, int32_t device, uint
 /* Device-resident batch, asynchronous on `stream` (a cudaStream_t, or NULL for the legacy
  * default stream): the kernel-only form of vdx_search_batch for callers whose queries and
  * results live in device memory. Per-query k and ef come from d_k / d_ef when not NULL, else
- * k_uniform / ef_uniform; result rows are out_stride wide. d_work is caller-owned device memory
+ * k_uniform / ef_uniform; result rows are out_stride wide (without d_k, out_stride must be at
+ * least k_uniform; with d_k, a row's count is cut to out_stride; each d_ef[i] must fit the result
+ * capacity the uniform ef sets, the next power of two >= max(ef_uniform, 32), else that row
+ * reports code 4). d_work is caller-owned device memory
  * of vdx_work_words() u32 words: [0] error code (0 = ok; 1 non-finite query, 2 zero cosine
  * query, 3 corrupt device graph, 4 ef above capacity), [1] the lowest failing row, [16..] the
  * 64-bit statistics words. The call does not wait for the kernel. The search runs as three
@@ -167,9 +178,13 @@ VDX_API vdx_status vdx_search_batch_device(const vdx_index* index, const float* 
  * (a launch needing more is rejected with VDX_ERR_LENGTH). The index must already have a
  * device copy for (opts->device, opts->precision): call vdx_index_upload first, which does
  * allocate. The first call on each device looks up the array's device address, so make it
- * before any stream capture. All calls share the array and clear it before their launch;
- * calls whose kernels overlap on the GPU race on it, so serialize them. Synchronous: returns
- * after the batch finished, with the reference's error for a bad query row. */
+ * before any stream capture; the address is kept for the life of the process, so resetting the
+ * device afterwards (cudaDeviceReset) is not supported. All calls share the array and clear it
+ * before their launch; calls whose kernels overlap on the GPU race on it, so serialize them.
+ * Synchronous: returns after the batch finished, with the reference's error for a bad query
+ * row. NULL query or result buffers (nq > 0), out_stride < k_uniform without d_k, and
+ * opts->learned_stop (its network needs device memory the index allocates) are rejected with
+ * VDX_ERR_INVALID_ARGUMENT before any launch. With d_k, a row's count never exceeds out_stride. */
 VDX_API vdx_status vdx_search_batch_device_noalloc(const vdx_index* index, const float* d_queries,
                                                    uint64_t nq, uint64_t dim, const uint32_t* d_k,
                                                    const uint32_t* d_ef, uint32_t k_uniform,

@@ -26,11 +26,17 @@ _U32 = ctypes.c_uint32
 _F = ctypes.c_float
 
 
+def ref_root() -> Path:
+    """The reference project's checkout: $REF_ROOT, else `reference` beside this repository."""
+    return Path(os.environ.get("REF_ROOT", HERE.parent.parent / "reference"))
+
+
 def build(ref: bool = True) -> None:
     """Compiles the restatement, and the reference when its sources are present."""
     subprocess.run(["make", "-s", "-C", str(HERE), "oracle"], check=True)
-    if ref and Path(os.environ.get("REF_ROOT", "/root/reference")).joinpath("src").exists():
-        subprocess.run(["make", "-s", "-C", str(HERE), "ref"], check=True)
+    root = ref_root()
+    if ref and root.joinpath("src").exists():
+        subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF_ROOT={root}"], check=True)
 
 
 def _p(a: np.ndarray) -> int:
