@@ -91,10 +91,8 @@ def reference_graph(base) -> Path:
 
 
 def recall_at_10(ids, truth) -> float:
-    hits = 0
-    for a, b in zip(ids, truth):
-        hits += len(set(a[:K].tolist()) & set(b[:K].tolist()))
-    return hits / (len(truth) * K)
+    from hnsw_vector_search_b200.recall import recall_at_k
+    return recall_at_k(ids, truth, K)
 
 
 class Clocks:

@@ -468,13 +468,13 @@ void HnswIndex::add_gpu(MatrixView<float> vectors, int device) {
     upper_.reserve(total);
     // Every vector stored (levels drawn in the serial order) before anything is linked.
     for (std::size_t r = 0; r < vectors.rows(); ++r) {
-        store(vectors.row(r));
+        append_node(vectors.row(r));
     }
     // The first nodes one by one on the host, exactly as the serial build.
     std::size_t next = first;
     const std::size_t seed_end = std::min(total, std::max<std::size_t>(first, dev::kSeedNodes));
     for (; next < seed_end; ++next) {
-        insert<Locking::None>(static_cast<Id>(next));
+        link_serial(static_cast<Id>(next));
     }
     if (next == total) {
         return;
@@ -649,7 +649,7 @@ void HnswIndex::add_gpu(MatrixView<float> vectors, int device) {
         gpu::check(cudaMemcpy(dev0.data(), dg.links0_alloc, dev0.size() * 4, cudaMemcpyDeviceToHost),
                    "download links");
         for (std::size_t v = first; v < total; ++v) {
-            Id* block = link_block(static_cast<Id>(v), 0);
+            Id* block = this->block(static_cast<Id>(v), 0).data();
             std::uint32_t c = 0;
             for (; c < cap0 && dev0[v * dg.view.stride0 + c] != dev::kNoId; ++c) {
                 block[1 + c] = dev0[v * dg.view.stride0 + c];
@@ -658,7 +658,7 @@ void HnswIndex::add_gpu(MatrixView<float> vectors, int device) {
         }
         // Old nodes' lists changed too (links back): copy every layer-0 list.
         for (std::size_t v = 0; v < first; ++v) {
-            Id* block = link_block(static_cast<Id>(v), 0);
+            Id* block = this->block(static_cast<Id>(v), 0).data();
             std::uint32_t c = 0;
             for (; c < cap0 && dev0[v * dg.view.stride0 + c] != dev::kNoId; ++c) {
                 block[1 + c] = dev0[v * dg.view.stride0 + c];
@@ -672,7 +672,7 @@ void HnswIndex::add_gpu(MatrixView<float> vectors, int device) {
             std::size_t b = 0;
             for (std::size_t v = 0; v < n; ++v) {
                 for (std::size_t l = 1; l <= levels_[v]; ++l, ++b) {
-                    Id* block = link_block(static_cast<Id>(v), l);
+                    Id* block = this->block(static_cast<Id>(v), l).data();
                     std::uint32_t c = 0;
                     for (; c < params_.M && devu[b * dg.view.stride_up + c] != dev::kNoId; ++c) {
                         block[1 + c] = devu[b * dg.view.stride_up + c];

@@ -180,34 +180,25 @@ public:
     std::size_t max_level() const noexcept { return max_level_; }
 
 private:
-    struct BuildLocks;
-    enum class Locking { None, PerNode };
+    struct ListGuards;  // mutexes of a parallel add (hnsw_build.cpp)
+    class Builder;      // the insertion procedure (hnsw_build.cpp)
 
     std::size_t max_links(std::size_t layer) const noexcept {
         return layer == 0 ? 2 * params_.M : params_.M;
     }
-    const Id* link_block(Id node, std::size_t layer) const noexcept;
-    Id* link_block(Id node, std::size_t layer) noexcept;
+    // A node's link block on `layer`: [count, ids...], 1 + max_links(layer) words.
+    std::span<Id> block(Id node, std::size_t layer) noexcept;
+    std::span<const Id> block(Id node, std::size_t layer) const noexcept;
+    // The links of a block (its first `count` ids); the count must be within capacity.
     std::span<const Id> links(Id node, std::size_t layer) const noexcept;
-    void set_links(Id node, std::size_t layer, std::span<const Neighbor> chosen) noexcept;
     float dist(const float* a, const float* b) const noexcept;
     const float* vector_of(Id node) const noexcept { return vectors_.row(node).data(); }
 
-    std::size_t random_level();
-    void store(std::span<const float> vector);
-    template <Locking L>
-    void insert(Id node);
-    template <Locking L>
-    void link_back(Id node, std::size_t layer, std::span<const Neighbor> chosen);
-    std::vector<Neighbor> select_neighbors(std::vector<Neighbor> candidates, std::size_t m) const;
-    template <Locking L>
-    Neighbor build_greedy(const float* query, Neighbor entry, std::size_t layer,
-                          std::vector<Id>& copy) const;
-    template <Locking L>
-    void build_search_layer(const float* query, Neighbor entry, std::size_t ef, std::size_t layer,
-                            struct BuildScratch& scratch) const;
-    template <Locking L>
-    std::span<const Id> read_links(Id node, std::size_t layer, std::vector<Id>& copy) const;
+    std::size_t draw_level();
+    // Stores a vector (normalized under cosine), draws its level and lays out empty link blocks.
+    void append_node(std::span<const float> vector);
+    // Inserts a stored node into the graph on the calling thread (the serial build's step).
+    void link_serial(Id node);
     void check_links(const std::filesystem::path& path) const;
     void invalidate_device() noexcept;
 
@@ -222,7 +213,7 @@ private:
     Id entry_point_ = 0;
     std::size_t max_level_ = 0;
 
-    std::unique_ptr<BuildLocks> build_locks_;
+    ListGuards* guards_ = nullptr;  // set only while a parallel add runs
     mutable std::unique_ptr<std::mutex> device_mutex_;
     mutable std::vector<std::unique_ptr<DeviceGraph>> device_;  // per (device, precision) slot
     StopModel stop_model_;

@@ -1,19 +1,39 @@
 // HnswIndex construction and diagnostics on the host.
 //
-// The graph must be the one the reference builds (src/hnsw.cpp:223-409 of the reference), so that
-// serial builds agree byte for byte and GPU results can be compared id for id: the level draw
-// (top 53 bits of mt19937_64, floor(-ln U / ln M)), the insertion procedure (greedy descent,
-// per-layer candidate search with ef = max(ef_construction, M), neighbor selection, links back)
-// and the selection heuristic are the same steps in the same order. The code is this project's
-// own. Parallel add() uses one lock per node, held one at a time, so no lock cycle can form.
+// The graph has to be the one the reference builds, so that a serial build here saves the same
+// file byte for byte and GPU results can be compared id for id with the reference's on either
+// build. What fixes the graph is the algorithm, which follows the HNSW paper (Malkov & Yashunin,
+// 2018) with the reference's choices (src/hnsw.cpp:223-409):
+//   * level of a new node: floor(-ln U * 1/ln M), U = 1 - (top 53 bits of the next mt19937_64
+//     output) * 2^-53, drawn when the vector is stored (paper Alg. 1, line 4);
+//   * insertion (Alg. 1): from the entry point, a greedy walk through the layers above the node's
+//     level, moving to the first strict minimum of each scanned neighbour list (distance only)
+//     until no move is made; then, on every layer from min(level, top) down to 0, a best-first
+//     search with ef = max(ef_construction, M) (Alg. 2) whose closest result seeds the next
+//     layer, and M neighbours selected from its results by the heuristic of Alg. 4 (no
+//     extension, no pruned-connection refill);
+//   * neighbour lists of the chosen nodes: the new node is appended while a list has room,
+//     otherwise the list is re-selected by the same heuristic from its old links plus the new
+//     node, at its capacity (2M on layer 0, M above);
+//   * order: (distance, id) as Neighbor's `closer` defines it, everywhere.
+//
+// How the code gets there is this project's own. The layer search keeps one sorted beam with an
+// "expanded" mark per entry instead of a candidate heap and a result heap: expanding the closest
+// unexpanded beam entry until none is left visits the same nodes in the same order and ends with
+// the same results (a candidate evicted from the results would only ever stop the heap search,
+// at the point where the beam has nothing left to expand). It is the same loop the GPU search
+// kernel runs. A parallel add stores every vector first (levels in the serial order), then
+// inserts the rest from worker threads that claim chunks of nodes; neighbour lists are guarded
+// by a fixed table of striped mutexes, at most one held at a time, and a node that raises the
+// top layer holds the entry-point mutex through its whole insertion.
 
 #include <algorithm>
 #include <atomic>
-#include <cassert>
 #include <cmath>
 #include <exception>
 #include <format>
 #include <mutex>
+#include <optional>
 #include <stdexcept>
 #include <thread>
 #include <utility>
@@ -24,37 +44,43 @@
 
 namespace vdx {
 
-struct HnswIndex::BuildLocks {
-    explicit BuildLocks(std::size_t n) : node(std::make_unique<std::mutex[]>(n)) {}
-    std::unique_ptr<std::mutex[]> node;  // guards that node's link blocks on every layer
-    std::mutex entry;                    // guards entry_point_ and max_level_
+// Mutexes of a parallel add: neighbour lists hash to one of a fixed number of stripes.
+struct HnswIndex::ListGuards {
+    static constexpr std::size_t kStripes = std::size_t{1} << 14;
+    std::mutex stripe[kStripes];
+    std::mutex top;  // entry point and top layer
+    std::mutex& of(Id node) noexcept { return stripe[(node * 0x9E3779B1u) >> 18]; }
 };
 
-// Per-insert scratch: visited stamps and the two heaps of the layer search.
-struct BuildScratch {
-    std::vector<std::uint32_t> stamp;
-    std::uint32_t epoch = 0;
-    std::vector<Neighbor> frontier;  // heap, closest on top
-    std::vector<Neighbor> best;      // heap, worst on top
-    std::vector<Id> fresh;
-    std::vector<Id> copy;
+// One inserting thread's procedure and scratch.
+class HnswIndex::Builder {
+public:
+    Builder(HnswIndex& index, ListGuards* guards) : ix_(index), guards_(guards) {}
 
-    void begin(std::size_t n) {
-        if (stamp.size() < n) {
-            stamp.resize(n, 0);
-        }
-        if (++epoch == 0) {
-            std::ranges::fill(stamp, 0U);
-            epoch = 1;
-        }
-    }
-    bool first_visit(Id id) noexcept {
-        if (stamp[id] == epoch) {
-            return false;
-        }
-        stamp[id] = epoch;
-        return true;
-    }
+    void insert(Id node);
+    const HnswIndex& index() const noexcept { return ix_; }
+    const ListGuards* guards() const noexcept { return guards_; }
+
+private:
+    struct Entry {
+        Neighbor n;
+        bool expanded;
+    };
+
+    std::span<const Id> neighbours(Id node, std::size_t layer);
+    Neighbor walk(const float* q, Neighbor at, std::size_t layer);
+    void layer_search(const float* q, Neighbor from, std::size_t ef, std::size_t layer);
+    std::vector<Neighbor> diverse(std::span<const Neighbor> sorted, std::size_t m) const;
+    void link_from(Id node, std::size_t layer, const Neighbor& to);
+    bool first_visit(Id id);
+
+    HnswIndex& ix_;
+    ListGuards* guards_;
+    std::vector<Id> list_copy_;
+    std::vector<std::uint32_t> mark_;
+    std::uint32_t epoch_ = 0;
+    std::vector<Entry> beam_;
+    std::vector<Neighbor> sorted_;
 };
 
 namespace {
@@ -73,109 +99,91 @@ HnswParams validated(const HnswParams& p) {
     return p;
 }
 
-// Heap orders for std heaps (greatest on top): `frontier` keeps the closest on top,
-// `best` keeps the worst on top.
-bool frontier_order(const Neighbor& a, const Neighbor& b) noexcept { return closer(b, a); }
-bool best_order(const Neighbor& a, const Neighbor& b) noexcept { return closer(a, b); }
-
-std::size_t thread_count(std::size_t requested) noexcept {
-    return requested != 0 ? requested : std::max(1U, std::thread::hardware_concurrency());
-}
-
-// fn(i) for i in [0, count) on `threads` threads claiming items from a shared counter; the first
-// exception is rethrown after all threads stop.
-template <typename Fn>
-void run_parallel(std::size_t count, std::size_t threads, const Fn& fn) {
-    if (count == 0) {
-        return;
-    }
-    std::atomic<std::size_t> next{0};
-    std::exception_ptr error;
-    std::mutex error_lock;
-    const auto worker = [&] {
+// Runs body(begin, end) over [0, count) on up to `threads` threads, each claiming chunks of 64
+// items; after every thread has stopped, the first error (in thread order) is rethrown.
+template <typename Body>
+void for_chunks(std::size_t count, std::size_t threads, const Body& body) {
+    constexpr std::size_t kChunk = 64;
+    std::atomic<std::size_t> cursor{0};
+    std::atomic<bool> failed{false};
+    const std::size_t workers = std::max<std::size_t>(1, std::min(threads, (count + kChunk - 1) / kChunk));
+    std::vector<std::optional<std::exception_ptr>> errors(workers);
+    const auto run = [&](std::size_t w) {
         try {
-            for (std::size_t i = next++; i < count; i = next++) {
-                fn(i);
+            while (!failed.load(std::memory_order_relaxed)) {
+                const std::size_t begin = cursor.fetch_add(kChunk);
+                if (begin >= count) {
+                    return;
+                }
+                body(begin, std::min(count, begin + kChunk));
             }
         } catch (...) {
-            next = count;
-            const std::scoped_lock lock(error_lock);
-            if (!error) {
-                error = std::current_exception();
-            }
+            errors[w] = std::current_exception();
+            failed = true;
         }
     };
-    std::vector<std::thread> pool;
-    for (std::size_t t = 1; t < std::min(threads, count); ++t) {
-        try {
-            pool.emplace_back(worker);
-        } catch (...) {
-            break;  // fewer threads: the work still gets done
+    {
+        std::vector<std::jthread> pool;
+        pool.reserve(workers - 1);
+        for (std::size_t w = 1; w < workers; ++w) {
+            pool.emplace_back(run, w);
         }
-    }
-    worker();
-    for (auto& t : pool) {
-        t.join();
-    }
-    if (error) {
-        std::rethrow_exception(error);
+        run(0);
+    }  // joins
+    for (const auto& e : errors) {
+        if (e) {
+            std::rethrow_exception(*e);
+        }
     }
 }
 
 }  // namespace
 
 HnswIndex::HnswIndex(std::size_t dim, Metric metric, HnswParams params)
-    : metric_(metric),
-      params_(validated(params)),
-      level_multiplier_(1.0 / std::log(static_cast<double>(params_.M))),
-      rng_(params_.seed),
-      vectors_(dim),
-      device_mutex_(std::make_unique<std::mutex>()) {}
+    : metric_(metric), params_(validated(params)), vectors_(dim) {
+    level_multiplier_ = 1.0 / std::log(static_cast<double>(params_.M));
+    rng_.seed(params_.seed);
+    device_mutex_ = std::make_unique<std::mutex>();
+}
 
 HnswIndex::~HnswIndex() = default;
 HnswIndex::HnswIndex(HnswIndex&&) noexcept = default;
 HnswIndex& HnswIndex::operator=(HnswIndex&&) noexcept = default;
 
-const Id* HnswIndex::link_block(Id node, std::size_t layer) const noexcept {
-    if (layer == 0) {
-        return layer0_.data() + static_cast<std::size_t>(node) * (1 + max_links(0));
-    }
-    return upper_[node].data() + (layer - 1) * (1 + max_links(layer));
+// Storage: layer 0 is one array of n blocks, every node's upper layers one vector of `level`
+// blocks; a block is [count, ids...] with room for max_links(layer) ids.
+std::span<const Id> HnswIndex::block(Id node, std::size_t layer) const noexcept {
+    const std::size_t width = 1 + max_links(layer);
+    const Id* base = layer == 0 ? layer0_.data() + static_cast<std::size_t>(node) * width
+                                : upper_[node].data() + (layer - 1) * width;
+    return {base, width};
 }
 
-Id* HnswIndex::link_block(Id node, std::size_t layer) noexcept {
-    return const_cast<Id*>(std::as_const(*this).link_block(node, layer));
+std::span<Id> HnswIndex::block(Id node, std::size_t layer) noexcept {
+    const std::span<const Id> b = std::as_const(*this).block(node, layer);
+    return {const_cast<Id*>(b.data()), b.size()};
 }
 
 std::span<const Id> HnswIndex::links(Id node, std::size_t layer) const noexcept {
-    const Id* block = link_block(node, layer);
-    return {block + 1, block[0]};
-}
-
-void HnswIndex::set_links(Id node, std::size_t layer, std::span<const Neighbor> chosen) noexcept {
-    Id* block = link_block(node, layer);
-    block[0] = static_cast<Id>(chosen.size());
-    for (std::size_t i = 0; i < chosen.size(); ++i) {
-        block[1 + i] = chosen[i].id;
-    }
+    const std::span<const Id> b = block(node, layer);
+    return b.subspan(1, b[0]);
 }
 
 float HnswIndex::dist(const float* a, const float* b) const noexcept {
-    if (metric_ == Metric::L2) {
-        return detail::l2_squared_raw(a, b, dim());
-    }
-    return 1.0F - detail::inner_product_raw(a, b, dim());
+    return metric_ == Metric::L2 ? detail::l2_squared_raw(a, b, dim())
+                                 : 1.0F - detail::inner_product_raw(a, b, dim());
 }
 
 std::size_t HnswIndex::memory_bytes() const noexcept {
-    // Every node's upper vector holds exactly level x (1 + M) ids (store() and load() size them
-    // so), which lets the levels give the total without visiting n separate allocations.
-    std::size_t blocks = 0;
+    // Every node's upper vector holds exactly level x (1 + M) ids (append_node() and load() size
+    // them so), which lets the levels give the total without visiting n separate allocations.
+    std::size_t upper_blocks = 0;
     for (const std::uint8_t level : levels_) {
-        blocks += level;
+        upper_blocks += level;
     }
     return vectors_.data().size_bytes() + levels_.size() + layer0_.size() * sizeof(Id) +
-           upper_.size() * sizeof(std::vector<Id>) + blocks * (1 + max_links(1)) * sizeof(Id);
+           upper_.size() * sizeof(std::vector<Id>) +
+           upper_blocks * (1 + max_links(1)) * sizeof(Id);
 }
 
 void HnswIndex::invalidate_device() noexcept {
@@ -185,32 +193,41 @@ void HnswIndex::invalidate_device() noexcept {
     }
 }
 
-// U = 1 - (top 53 bits) * 2^-53 lies in (0, 1]; level = floor(-ln U * mL).
-std::size_t HnswIndex::random_level() {
-    const double u = 1.0 - static_cast<double>(rng_() >> 11U) * 0x1.0p-53;
+std::size_t HnswIndex::draw_level() {
+    const std::uint64_t top53 = rng_() >> 11U;
+    const double u = 1.0 - std::ldexp(static_cast<double>(top53), -53);  // in (0, 1]
     return static_cast<std::size_t>(-std::log(u) * level_multiplier_);
 }
 
-void HnswIndex::store(std::span<const float> vector) {
-    if (!device_mutex_) {  // moved-from index being reused
+void HnswIndex::append_node(std::span<const float> vector) {
+    if (device_mutex_ == nullptr) {  // a moved-from index being reused
         device_mutex_ = std::make_unique<std::mutex>();
     }
+    const std::size_t id = size();
     vectors_.append(vector);
     if (metric_ == Metric::Cosine) {
-        detail::normalize(vectors_.row(size() - 1));
+        detail::normalize(vectors_.row(id));
     }
-    const std::size_t level = random_level();
+    const std::size_t level = draw_level();
     levels_.push_back(static_cast<std::uint8_t>(level));
-    layer0_.resize(layer0_.size() + 1 + max_links(0), Id{0});
-    upper_.emplace_back(level * (1 + max_links(1)), Id{0});
+    layer0_.insert(layer0_.end(), 1 + max_links(0), Id{0});
+    upper_.push_back(std::vector<Id>(level * (1 + max_links(1)), Id{0}));
+}
+
+void HnswIndex::link_serial(Id node) {
+    thread_local std::unique_ptr<Builder> builder;
+    if (builder == nullptr || &builder->index() != this) {
+        builder = std::make_unique<Builder>(*this, nullptr);
+    }
+    builder->insert(node);
 }
 
 Id HnswIndex::add(std::span<const float> vector) {
     detail::check_new_vectors("HnswIndex::add", {metric_, dim(), size()}, vector.size(), vector);
     invalidate_device();
-    store(vector);
+    append_node(vector);
     const auto id = static_cast<Id>(size() - 1);
-    insert<Locking::None>(id);
+    link_serial(id);
     return id;
 }
 
@@ -222,205 +239,234 @@ void HnswIndex::add(MatrixView<float> vectors, std::size_t num_threads) {
     detail::check_new_vectors("HnswIndex::add", {metric_, dim(), size()}, vectors.dim(),
                               vectors.data());
     invalidate_device();
+    const std::size_t rows = vectors.rows();
     const std::size_t first = size();
-    const std::size_t total = first + vectors.rows();
-    vectors_.reserve_rows(total);
-    levels_.reserve(total);
-    layer0_.reserve(total * (1 + max_links(0)));
-    upper_.reserve(total);
-    const std::size_t threads = std::min(thread_count(num_threads), vectors.rows());
-    if (threads <= 1) {
-        for (std::size_t r = 0; r < vectors.rows(); ++r) {
-            store(vectors.row(r));
-            insert<Locking::None>(static_cast<Id>(size() - 1));
+    vectors_.reserve_rows(first + rows);
+    levels_.reserve(first + rows);
+    layer0_.reserve((first + rows) * (1 + max_links(0)));
+    upper_.reserve(first + rows);
+    const std::size_t threads =
+        num_threads == 0 ? std::max(1U, std::thread::hardware_concurrency()) : num_threads;
+    if (threads == 1 || rows <= 1) {
+        for (std::size_t r = 0; r < rows; ++r) {
+            append_node(vectors.row(r));
+            link_serial(static_cast<Id>(first + r));
         }
         return;
     }
-    // Every vector is stored (levels drawn in serial order) before any is linked, so no container
-    // grows while other threads read it.
-    build_locks_ = std::make_unique<BuildLocks>(total);
-    for (std::size_t r = 0; r < vectors.rows(); ++r) {
-        store(vectors.row(r));
+    // All vectors stored (and levels drawn in the serial order) before any link is made, so no
+    // container is resized while workers read it.
+    for (std::size_t r = 0; r < rows; ++r) {
+        append_node(vectors.row(r));
     }
-    std::size_t next = first;
-    if (next == 0) {
-        insert<Locking::None>(0);
-        next = 1;
+    std::size_t start = first;
+    if (start == 0) {
+        link_serial(0);  // the first node only becomes the entry point
+        start = 1;
     }
-    run_parallel(total - next, threads,
-                 [this, next](std::size_t i) { insert<Locking::PerNode>(static_cast<Id>(next + i)); });
-    build_locks_.reset();
+    auto guards = std::make_unique<ListGuards>();
+    guards_ = guards.get();
+    try {
+        for_chunks(size() - start, threads, [&](std::size_t begin, std::size_t end) {
+            thread_local std::unique_ptr<Builder> builder;
+            if (builder == nullptr || &builder->index() != this || builder->guards() != guards_) {
+                builder = std::make_unique<Builder>(*this, guards_);
+            }
+            for (std::size_t i = begin; i < end; ++i) {
+                builder->insert(static_cast<Id>(start + i));
+            }
+        });
+    } catch (...) {
+        guards_ = nullptr;
+        throw;
+    }
+    guards_ = nullptr;
 }
 
-template <HnswIndex::Locking L>
-std::span<const Id> HnswIndex::read_links(Id node, std::size_t layer,
-                                          std::vector<Id>& copy) const {
-    if constexpr (L == Locking::PerNode) {
-        const std::scoped_lock lock(build_locks_->node[node]);
-        const auto ids = links(node, layer);
-        copy.assign(ids.begin(), ids.end());
-        return copy;
-    } else {
-        return links(node, layer);
+// ---------------------------------------------------------------------------------------------
+// The insertion procedure.
+
+bool HnswIndex::Builder::first_visit(Id id) {
+    if (mark_[id] == epoch_) {
+        return false;
     }
+    mark_[id] = epoch_;
+    return true;
 }
 
-template <HnswIndex::Locking L>
-Neighbor HnswIndex::build_greedy(const float* query, Neighbor entry, std::size_t layer,
-                                 std::vector<Id>& copy) const {
-    bool moved = true;
-    while (moved) {
-        moved = false;
-        for (const Id id : read_links<L>(entry.id, layer, copy)) {
-            const float d = dist(query, vector_of(id));
-            if (d < entry.distance) {
-                entry = {d, id};
-                moved = true;
+// A node's neighbour list on `layer`; under a parallel add a copy taken under its stripe.
+std::span<const Id> HnswIndex::Builder::neighbours(Id node, std::size_t layer) {
+    if (guards_ == nullptr) {
+        return ix_.links(node, layer);
+    }
+    const std::scoped_lock lock(guards_->of(node));
+    const std::span<const Id> now = ix_.links(node, layer);
+    list_copy_.assign(now.begin(), now.end());
+    return list_copy_;
+}
+
+// Greedy walk on one layer: score the whole list of the current node, move to its first strict
+// minimum if that beats the current distance, repeat until no move.
+Neighbor HnswIndex::Builder::walk(const float* q, Neighbor at, std::size_t layer) {
+    for (;;) {
+        Neighbor best = at;
+        for (const Id id : neighbours(at.id, layer)) {
+            const float d = ix_.dist(q, ix_.vector_of(id));
+            if (d < best.distance) {
+                best = {d, id};
             }
         }
+        if (best.id == at.id) {
+            return at;
+        }
+        at = best;
     }
-    return entry;
 }
 
-template <HnswIndex::Locking L>
-void HnswIndex::build_search_layer(const float* query, Neighbor entry, std::size_t ef,
-                                   std::size_t layer, BuildScratch& s) const {
-    s.begin(size());
-    s.first_visit(entry.id);
-    s.frontier.assign(1, entry);
-    s.best.assign(1, entry);
-    while (!s.frontier.empty()) {
-        std::ranges::pop_heap(s.frontier, frontier_order);
-        const Neighbor current = s.frontier.back();
-        s.frontier.pop_back();
-        if (s.best.size() >= ef && closer(s.best.front(), current)) {
-            break;
+// Best-first search of one layer into beam_: at most ef entries, sorted by `closer`.
+void HnswIndex::Builder::layer_search(const float* q, Neighbor from, std::size_t ef,
+                                      std::size_t layer) {
+    if (mark_.size() < ix_.size()) {
+        mark_.resize(ix_.size(), 0);
+    }
+    if (++epoch_ == 0) {
+        std::ranges::fill(mark_, 0U);
+        epoch_ = 1;
+    }
+    first_visit(from.id);
+    beam_.assign(1, Entry{from, false});
+    std::size_t cursor = 0;  // no unexpanded entry before this position
+    for (;;) {
+        while (cursor < beam_.size() && beam_[cursor].expanded) {
+            ++cursor;
         }
-        s.fresh.clear();
-        for (const Id id : read_links<L>(current.id, layer, s.copy)) {
-            if (s.first_visit(id)) {
-                s.fresh.push_back(id);
+        if (cursor == beam_.size()) {
+            return;
+        }
+        beam_[cursor].expanded = true;
+        const Id node = beam_[cursor].n.id;
+        for (const Id id : neighbours(node, layer)) {
+            if (!first_visit(id)) {
+                continue;
             }
-        }
-        for (const Id id : s.fresh) {
-            const Neighbor n{dist(query, vector_of(id)), id};
-            if (s.best.size() < ef || closer(n, s.best.front())) {
-                s.frontier.push_back(n);
-                std::ranges::push_heap(s.frontier, frontier_order);
-                s.best.push_back(n);
-                std::ranges::push_heap(s.best, best_order);
-                if (s.best.size() > ef) {
-                    std::ranges::pop_heap(s.best, best_order);
-                    s.best.pop_back();
-                }
+            const Neighbor cand{ix_.dist(q, ix_.vector_of(id)), id};
+            const bool full = beam_.size() >= ef;
+            if (full && !closer(cand, beam_.back().n)) {
+                continue;
             }
+            const auto at = std::ranges::upper_bound(beam_, cand, closer, &Entry::n);
+            const auto pos = static_cast<std::size_t>(at - beam_.begin());
+            beam_.insert(at, Entry{cand, false});
+            if (full) {
+                beam_.pop_back();
+            }
+            cursor = std::min(cursor, pos);
         }
     }
 }
 
-template <HnswIndex::Locking L>
-void HnswIndex::insert(Id node) {
-    const std::size_t level = levels_[node];
-    if (node == 0) {
-        entry_point_ = 0;
-        max_level_ = level;
-        return;
-    }
-    std::unique_lock<std::mutex> entry_lock;
-    if constexpr (L == Locking::PerNode) {
-        entry_lock = std::unique_lock(build_locks_->entry);
-    }
-    const Id entry_point = entry_point_;
-    const std::size_t max_level = max_level_;
-    if (entry_lock.owns_lock() && level <= max_level) {
-        entry_lock.unlock();  // only a node raising the top layer keeps it
-    }
-    thread_local BuildScratch scratch;
-    const float* query = vector_of(node);
-    Neighbor entry{dist(query, vector_of(entry_point)), entry_point};
-    for (std::size_t layer = max_level; layer > level; --layer) {
-        entry = build_greedy<L>(query, entry, layer, scratch.copy);
-    }
-    const std::size_t ef = std::max(params_.ef_construction, params_.M);
-    const std::size_t top = std::min(level, max_level);
-    std::vector<std::vector<Neighbor>> chosen(top + 1);
-    for (std::size_t i = 0; i <= top; ++i) {
-        const std::size_t layer = top - i;
-        build_search_layer<L>(query, entry, ef, layer, scratch);
-        entry = *std::ranges::min_element(scratch.best, closer);
-        chosen[layer] = select_neighbors(scratch.best, params_.M);
-    }
-    {
-        std::unique_lock<std::mutex> own;
-        if constexpr (L == Locking::PerNode) {
-            own = std::unique_lock(build_locks_->node[node]);
-        }
-        for (std::size_t layer = 0; layer <= top; ++layer) {
-            set_links(node, layer, chosen[layer]);
-        }
-    }
-    for (std::size_t layer = 0; layer <= top; ++layer) {
-        link_back<L>(node, layer, chosen[layer]);
-    }
-    if (level > max_level) {
-        max_level_ = level;
-        entry_point_ = node;
-    }
-}
-
-template <HnswIndex::Locking L>
-void HnswIndex::link_back(Id node, std::size_t layer, std::span<const Neighbor> chosen) {
-    for (const Neighbor& n : chosen) {
-        std::unique_lock<std::mutex> lock;
-        if constexpr (L == Locking::PerNode) {
-            lock = std::unique_lock(build_locks_->node[n.id]);
-        }
-        Id* block = link_block(n.id, layer);
-        const std::size_t count = block[0];
-        if (count < max_links(layer)) {
-            block[1 + count] = node;
-            block[0] = static_cast<Id>(count + 1);
-            continue;
-        }
-        std::vector<Neighbor> candidates;
-        candidates.reserve(count + 1);
-        const float* base = vector_of(n.id);
-        for (const Id id : links(n.id, layer)) {
-            candidates.push_back({dist(base, vector_of(id)), id});
-        }
-        candidates.push_back({n.distance, node});
-        set_links(n.id, layer, select_neighbors(std::move(candidates), max_links(layer)));
-    }
-}
-
-// Keep a candidate (closest first) only if it is closer to the base node than to every
-// candidate already kept; with m or fewer candidates keep all.
-std::vector<Neighbor> HnswIndex::select_neighbors(std::vector<Neighbor> candidates,
+// Paper Alg. 4 over candidates sorted by `closer`: a candidate is kept unless some kept node is
+// closer to it than the base node is; at most m kept; m or fewer candidates are all kept.
+std::vector<Neighbor> HnswIndex::Builder::diverse(std::span<const Neighbor> sorted,
                                                   std::size_t m) const {
-    std::ranges::sort(candidates, closer);
-    if (candidates.size() <= m) {
-        return candidates;
+    if (sorted.size() <= m) {
+        return {sorted.begin(), sorted.end()};
     }
     std::vector<Neighbor> kept;
     kept.reserve(m);
-    for (const Neighbor& c : candidates) {
-        if (kept.size() == m) {
-            break;
-        }
-        const float* v = vector_of(c.id);
-        bool diverse = true;
-        for (const Neighbor& k : kept) {
-            if (dist(v, vector_of(k.id)) < c.distance) {
-                diverse = false;
-                break;
-            }
-        }
-        if (diverse) {
-            kept.push_back(c);
+    for (std::size_t i = 0; i < sorted.size() && kept.size() < m; ++i) {
+        const float* v = ix_.vector_of(sorted[i].id);
+        const bool dominated = std::ranges::any_of(kept, [&](const Neighbor& k) {
+            return ix_.dist(v, ix_.vector_of(k.id)) < sorted[i].distance;
+        });
+        if (!dominated) {
+            kept.push_back(sorted[i]);
         }
     }
     return kept;
 }
+
+// Adds `node` (at distance to.distance) to the list of `to.id` on `layer`: appended while the
+// list has room, else the list is re-selected from its links plus `node`.
+void HnswIndex::Builder::link_from(Id node, std::size_t layer, const Neighbor& to) {
+    std::unique_lock<std::mutex> lock;
+    if (guards_ != nullptr) {
+        lock = std::unique_lock(guards_->of(to.id));
+    }
+    const std::span<Id> b = ix_.block(to.id, layer);
+    const std::size_t cap = ix_.max_links(layer);
+    if (b[0] < cap) {
+        b[1 + b[0]] = node;
+        ++b[0];
+        return;
+    }
+    const float* owner = ix_.vector_of(to.id);
+    sorted_.clear();
+    for (std::size_t i = 1; i <= b[0]; ++i) {
+        sorted_.push_back({ix_.dist(owner, ix_.vector_of(b[i])), b[i]});
+    }
+    sorted_.push_back({to.distance, node});
+    std::ranges::sort(sorted_, closer);
+    const std::vector<Neighbor> kept = diverse(sorted_, cap);
+    b[0] = static_cast<Id>(kept.size());
+    std::ranges::transform(kept, b.begin() + 1, &Neighbor::id);
+}
+
+void HnswIndex::Builder::insert(Id node) {
+    const std::size_t level = ix_.levels_[node];
+    if (node == 0) {
+        ix_.entry_point_ = 0;
+        ix_.max_level_ = level;
+        return;
+    }
+    std::unique_lock<std::mutex> top;
+    if (guards_ != nullptr) {
+        top = std::unique_lock(guards_->top);
+    }
+    const Id entry = ix_.entry_point_;
+    const std::size_t top_level = ix_.max_level_;
+    const bool raises_top = level > top_level;
+    if (top.owns_lock() && !raises_top) {
+        top.unlock();
+    }
+    const float* q = ix_.vector_of(node);
+    Neighbor at{ix_.dist(q, ix_.vector_of(entry)), entry};
+    for (std::size_t layer = top_level; layer > level; --layer) {
+        at = walk(q, at, layer);
+    }
+    const std::size_t ef = std::max(ix_.params_.ef_construction, ix_.params_.M);
+    const std::size_t highest = std::min(level, top_level);
+    std::vector<std::vector<Neighbor>> chosen(highest + 1);
+    for (std::size_t layer = highest + 1; layer-- > 0;) {
+        layer_search(q, at, ef, layer);
+        at = beam_.front().n;
+        sorted_.clear();
+        std::ranges::transform(beam_, std::back_inserter(sorted_), &Entry::n);
+        chosen[layer] = diverse(sorted_, ix_.params_.M);
+    }
+    {
+        std::unique_lock<std::mutex> own;
+        if (guards_ != nullptr) {
+            own = std::unique_lock(guards_->of(node));
+        }
+        for (std::size_t layer = 0; layer <= highest; ++layer) {
+            const std::span<Id> b = ix_.block(node, layer);
+            b[0] = static_cast<Id>(chosen[layer].size());
+            std::ranges::transform(chosen[layer], b.begin() + 1, &Neighbor::id);
+        }
+    }
+    for (std::size_t layer = 0; layer <= highest; ++layer) {
+        for (const Neighbor& to : chosen[layer]) {
+            link_from(node, layer, to);
+        }
+    }
+    if (raises_top) {
+        ix_.max_level_ = level;
+        ix_.entry_point_ = node;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
 
 GraphReport HnswIndex::inspect() const {
     GraphReport r;

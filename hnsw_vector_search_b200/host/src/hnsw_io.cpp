@@ -328,7 +328,7 @@ void HnswIndex::check_links(const std::filesystem::path& path) const {
     for (Id node = 0; node < n; ++node) {
         const std::size_t level = levels_[node];
         for (std::size_t layer = 0; layer <= level; ++layer) {
-            const std::size_t count = link_block(node, layer)[0];
+            const std::size_t count = block(node, layer)[0];
             if (count > max_links(layer)) {
                 fail(path, std::format("node {} has {} links on layer {} (max {})", node, count,
                                        layer, max_links(layer)));

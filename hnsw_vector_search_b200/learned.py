@@ -26,6 +26,7 @@ from pathlib import Path
 import numpy as np
 
 from . import _P, _U32, _U64, _raise, _ptr, lib
+from .recall import recall_at_k
 
 FEATURES = 12
 PARAMS = 5057
@@ -157,8 +158,7 @@ def attach(index, model: StopModel) -> None:
 
 
 def recall(ids: np.ndarray, truth: np.ndarray, k: int) -> float:
-    hits = sum(len(set(a[:k].tolist()) & set(b[:k].tolist())) for a, b in zip(ids, truth))
-    return hits / (len(truth) * k)
+    return recall_at_k(ids, truth, k)
 
 
 def calibrate(index, model: StopModel, queries: np.ndarray, truth: np.ndarray, k: int,

@@ -94,6 +94,21 @@ def test_serial_build_matches_reference_on_real_valued_data(vdx, orc, tmp_path, 
     assert vdx.HnswIndex.load(tmp_path / "ref.vdx").info()["memory_bytes"] == ref.info()["memory_bytes"]
 
 
+@pytest.mark.parametrize("metric", [0, 1, 2])
+def test_serial_build_matches_reference_under_heavy_ties(vdx, orc, tmp_path, metric):
+    """Values in {1, 2, 3} over 6 dims: most distances tie, so every choice the build makes
+    between equal distances (beam order, eviction, the heuristic's strict test, the greedy walk's
+    first strict minimum) shows in the saved file."""
+    base = np.random.default_rng(11).integers(1, 4, size=(1500, 6)).astype(np.float32)
+    ref = orc.RefHnsw(6, metric, 4, 20, 3)
+    ref.add(base, threads=1)
+    ref.save(tmp_path / "ref.vdx")
+    mine = vdx.HnswIndex(6, metric, M=4, ef_construction=20, seed=3)
+    mine.add(base, num_threads=1)
+    mine.save(tmp_path / "mine.vdx")
+    assert (tmp_path / "mine.vdx").read_bytes() == (tmp_path / "ref.vdx").read_bytes()
+
+
 def test_files_round_trip_both_ways(vdx, orc, tmp_path):
     mine = vdx.HnswIndex.load(GOLDEN / "kat_m8.vdx")
     mine.save(tmp_path / "again.vdx")
