@@ -282,7 +282,7 @@ def main():
                     help="one search launch per warm-up step on the cached workload (for ncu)")
     ap.add_argument("--mode", default="fp32", choices=["fp32", "bf16", "fp8", "bf_tc", "bf_exact"])
     ap.add_argument("--ef", type=int, default=32)
-    ap.add_argument("--study", choices=["uneven", "precision", "build", "device_image"],
+    ap.add_argument("--study", choices=["uneven", "precision", "build", "device_image", "learned"],
                     help="instead of the headline: the uneven-batch stream or the precision study")
     ap.add_argument("--rows", type=int, default=0, help="base rows of a study (0: its default)")
     args = ap.parse_args()
@@ -322,6 +322,9 @@ def main():
     if args.study == "build":
         study_build(args, v, torch)
         return
+    if args.study == "learned":
+        study_learned(args, v, torch)
+        return
     base, queries = workload()
     cpu = None
     if rank == 0:
@@ -335,9 +338,10 @@ def main():
     modes = [("fp32", {}), ("bf16", {"precision": "bf16", "rerank": 40})]
     for _, o in modes:
         ix.upload(local, o.get("precision", "fp32"))
-    learned_info = learned_mode(v, ix, base, graph, local)
+    learned_info = learned_mode(v, torch, ix, base, graph, local)
     modes.append(("learned_bf16", {"precision": "bf16", "rerank": 40, "learned_stop": True,
-                                   "stop_threshold": learned_info["threshold"]}))
+                                   "stop_threshold": learned_info["threshold"],
+                                   "stop_gate": learned_info["gate"]}))
 
     # Operating points: the smallest swept ef reaching recall 0.95, per mode.
     points = {}
@@ -459,6 +463,7 @@ def main():
             e2e_kernels = int(v.lib().vdx_search_kernels_last())  # one end-to-end call's launches
 
     parity = parity_section(v, ix, graph, queries, truth, local, learned_info) if rank == 0 else None
+    analysis = learned_analysis(v, torch, ix, queries, results, learned_info, local) if rank == 0 else None
     brute = bruteforce_section(v, torch, base, queries, dev) if rank == 0 else None
     if rank == 0:
         cpu = cpu_baseline(graph, queries, results["fp32"]["ef"])
@@ -481,6 +486,7 @@ def main():
                            "recall_at_10": round(results["fp32"]["recall"], 4)},
             "speedup_vs_plain_fp32": r["qps"] / results["fp32"]["qps"],
             "learned": learned_info,
+            "learned_analysis": analysis,
             "modes": {n: {"qps": x["qps"], "ef": x["ef"], "recall_at_10": round(x["recall"], 4),
                           "speedup_vs_plain_fp32": x["qps"] / results["fp32"]["qps"]}
                       for n, x in results.items()},
@@ -556,19 +562,56 @@ def parity_section(v, ix, graph, queries, truth, device, learned_info) -> dict:
     if cap:
         rid, _, _ = ref.search_batch(queries, K, cap, threads)
         gid, _, _ = ix.search_batch(queries, K, cap, device=device, precision="bf16", rerank=40,
-                                    learned_stop=True, stop_threshold=learned_info["threshold"])
+                                    learned_stop=True, stop_threshold=learned_info["threshold"],
+                                    stop_gate=learned_info["gate"])
         out["learned_bf16"] = {"ef_cap": cap, "recall": round(recall_at_10(gid, truth), 4),
                                "reference_recall_at_cap": round(recall_at_10(rid, truth), 4)}
     return out
 
 
-def learned_mode(v, ix, base, graph, device) -> dict:
-    """Trains (or loads the cached) learned-termination model for this graph. For each candidate
-    ef cap: traces of the plain search at that cap for 20,000 training queries (seed 21, the
-    same mixture as the test queries) judged by exact brute force, this library's training
-    kernels, then the stop threshold calibrated on 5,000 more queries (seed 22) for
-    recall@10 >= 0.955 with BF16 traversal; the cap whose calibrated search reads the fewest
-    bytes wins. The 10,000 test queries are never used for training or calibration."""
+LEARNED_CAPS = (40, 44, 48, 56, 64)  # result capacity 64: the register-beam kernels
+LEARNED_GATES = (0, 2)
+CAL_TARGET = 0.955
+
+
+def device_ms(v, torch, ix, queries_dev, ef, reps=5, **opts) -> tuple[float, dict]:
+    """Median CUDA-event time (ms) of one device search of `queries_dev` (on the current stream,
+    after two untimed runs) and that search's statistics words."""
+    dev = queries_dev.device
+    nq = queries_dev.shape[0]
+    ids = torch.empty((nq, K), dtype=torch.int32, device=dev)
+    d = torch.empty((nq, K), dtype=torch.float32, device=dev)
+    c = torch.empty(nq, dtype=torch.int32, device=dev)
+    work = torch.zeros(int(v.lib().vdx_work_words()), dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    times = []
+    for i in range(reps + 2):
+        start = torch.cuda.Event(enable_timing=True)
+        end = torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        ix.search_batch_device(queries_dev, K, ef, K, ids, d, c, work, stream=stream.cuda_stream,
+                               device=dev.index, **opts)
+        end.record(stream)
+        end.synchronize()
+        if i >= 2:
+            times.append(start.elapsed_time(end))
+    st = work[16:16 + 2 * 10].cpu().numpy().view(np.uint64)
+    names = ["queries", "expansions", "dist_layer0", "dist_upper", "link_bytes", "row_bytes",
+             "rerank_bytes", "duplicates", "prefetch_hits", "learned_stops"]
+    return float(np.median(times)), {n: int(x) for n, x in zip(names, st)}
+
+
+def learned_mode(v, torch, ix, base, graph, device) -> dict:
+    """Trains (or loads the cached) learned-termination model for this graph and picks how to
+    run it, never looking at the 10,000 test queries. For each candidate ef cap (result capacity
+    <= 64, so the register-beam kernels run): traces of the plain search at that cap for 20,000
+    training queries (seed 21, the same mixture as the test queries) judged by exact brute
+    force, this library's training kernels, then for each gate (0: consult the network at every
+    checkpoint; 2: only once the k-th distance has been unchanged for 2 expansions) the stop
+    threshold calibrated on 5,000 more queries (seed 22) for recall@10 >= 0.955 with BF16
+    traversal. The candidate whose calibrated search of the calibration queries takes the least
+    device time wins; the plain BF16 search's time at its own smallest ef reaching 0.955 on the
+    same queries is reported beside it."""
     from hnsw_vector_search_b200 import learned
     from hnsw_vector_search_b200.datasets import integer_clusters
     path = CACHE / (graph.stem + f"_stop_model_v{learned.MODEL_VERSION}.npz")
@@ -584,33 +627,79 @@ def learned_mode(v, ix, base, graph, device) -> dict:
         cal_q = integer_clusters(CAL_QUERIES, 128, 1000, seed=22, centers_seed=111)
         train_truth, _, _ = bf.search_batch(train_q, K, method="tensor_core")
         cal_truth, _, _ = bf.search_batch(cal_q, K, method="tensor_core")
+        del bf
+        cal_dev = torch.from_numpy(cal_q).to(torch.device("cuda", device))
+        bf16 = {"precision": "bf16", "rerank": 40}
+        plain_ef = EF_SWEEP[-1]
+        for ef in EF_SWEEP:
+            ids, _, _ = ix.search_batch(cal_q, K, ef, device=device, **bf16)
+            if recall_at_10(ids, cal_truth) >= CAL_TARGET:
+                plain_ef = ef
+                break
+        plain_ms, _ = device_ms(v, torch, ix, cal_dev, plain_ef, **bf16)
         best = None
         tried = []
-        for cap in (40, 48, 64, 96):
+        for cap in LEARNED_CAPS:
             tr = learned.traces(ix, train_q, train_truth, k=K, ef=cap, device=device)
             x, y = learned.training_set(tr)
-            model_c, losses = learned.train(x, y, tr["proj"], epochs=6)
-            thr, rec = learned.calibrate(ix, model_c, cal_q, cal_truth, K, 0.955, cap,
-                                         precision="bf16", rerank=40, device=device)
-            ix.search_batch(cal_q, K, cap, precision="bf16", rerank=40, learned_stop=True,
-                            stop_threshold=thr, device=device)
-            work = v.HnswIndex.last_stats()["row_bytes"]
-            tried.append({"ef_cap": cap, "threshold": thr, "calibration_recall": round(rec, 4),
-                          "row_bytes": int(work), "samples": int(len(x)),
-                          "positive_share": round(float(y.mean()), 3)})
-            if rec >= 0.955 and (best is None or work < best[2]):
-                best = (thr, cap, work, rec, model_c)
+            model_c, _ = learned.train(x, y, tr["proj"], epochs=6)
+            for gate in LEARNED_GATES:
+                thr, rec = learned.calibrate(ix, model_c, cal_q, cal_truth, K, CAL_TARGET, cap,
+                                             precision="bf16", rerank=40, device=device,
+                                             stop_gate=gate)
+                ms, st = device_ms(v, torch, ix, cal_dev, cap, learned_stop=True,
+                                   stop_threshold=thr, stop_gate=gate, **bf16)
+                tried.append({"ef_cap": cap, "gate": gate, "threshold": thr,
+                              "calibration_recall": round(rec, 4), "calibration_ms": round(ms, 4),
+                              "dist_layer0": st["dist_layer0"], "stops": st["learned_stops"],
+                              "samples": int(len(x)), "positive_share": round(float(y.mean()), 3)})
+                if rec >= CAL_TARGET and (best is None or ms < best[2]):
+                    best = (thr, cap, ms, rec, gate, model_c)
         if best is None:
-            best = (tried[-1]["threshold"], 96, 0, tried[-1]["calibration_recall"], model_c)
-        model = best[4]
-        model.threshold, model.ef_cap = best[0], best[1]
+            t = tried[-1]
+            best = (t["threshold"], t["ef_cap"], t["calibration_ms"], t["calibration_recall"],
+                    t["gate"], model_c)
+        model = best[5]
+        model.threshold, model.ef_cap, model.gate = best[0], best[1], best[4]
         model.save(path)
         info.update({"source": "trained", "train_seconds": round(time.time() - t0, 1),
-                     "candidates": tried, "calibration_recall": round(best[3], 4)})
+                     "candidates": tried, "calibration_recall": round(best[3], 4),
+                     "calibration_ms": round(best[2], 4),
+                     "plain_bf16_on_calibration": {"ef": plain_ef, "ms": round(plain_ms, 4)}})
     learned.attach(ix, model)
-    info.update({"threshold": model.threshold, "ef_cap": model.ef_cap,
-                 "train_queries": TRAIN_QUERIES, "calibration_queries": CAL_QUERIES})
+    info.update({"threshold": model.threshold, "ef_cap": model.ef_cap, "gate": model.gate,
+                 "train_queries": TRAIN_QUERIES, "calibration_queries": CAL_QUERIES,
+                 "labels": "traces at the ef cap: a checkpoint is converged when its top-10 hits "
+                           "already equal the search's final hits"})
     return info
+
+
+def learned_analysis(v, torch, ix, queries, results, learned_info, device) -> dict:
+    """What the learned stop saves and what it costs, on the test queries, all device-timed on
+    one stream: the calibrated learned search; the same kernel with a threshold it never reaches
+    (every check paid, no stop); the plain BF16 search at the learned cap and at its own
+    operating ef. checks = checkpoints at which the network ran (gate permitting) is bounded by
+    expansions / 8."""
+    q = torch.from_numpy(queries).to(torch.device("cuda", device))
+    cap, gate, thr = learned_info["ef_cap"], learned_info["gate"], learned_info["threshold"]
+    bf16 = {"precision": "bf16", "rerank": 40}
+    out = {}
+    out["learned"] = device_ms(v, torch, ix, q, cap, learned_stop=True, stop_threshold=thr,
+                               stop_gate=gate, **bf16)
+    out["learned_never_stops"] = device_ms(v, torch, ix, q, cap, learned_stop=True,
+                                           stop_threshold=2.0, stop_gate=gate, **bf16)
+    out["plain_at_cap"] = device_ms(v, torch, ix, q, cap, **bf16)
+    ef0 = results["bf16"]["ef"]
+    out["plain_at_operating_ef"] = device_ms(v, torch, ix, q, ef0, **bf16)
+    rows = {k: {"ms": round(ms, 4), **st} for k, (ms, st) in out.items()}
+    never, plain_cap = out["learned_never_stops"], out["plain_at_cap"]
+    checkpoints = max(1, never[1]["expansions"] // 8)
+    return {"ef_cap": cap, "gate": gate, "threshold": thr, "operating_ef_plain": ef0, "runs": rows,
+            "check_overhead_frac": (never[0] - plain_cap[0]) / plain_cap[0],
+            "check_cost_ns_upper_bound": (never[0] - plain_cap[0]) * 1e6 / checkpoints,
+            "dist_saved_vs_plain_at_cap": 1.0 - out["learned"][1]["dist_layer0"] / plain_cap[1]["dist_layer0"],
+            "dist_ratio_vs_plain_at_operating_ef":
+                out["learned"][1]["dist_layer0"] / out["plain_at_operating_ef"][1]["dist_layer0"]}
 
 
 def bruteforce_section(v, torch, base, queries, dev) -> dict:
@@ -705,14 +794,34 @@ def study_uneven(args, v, torch):
     n = args.rows or 1_000_000
     CACHE.mkdir(exist_ok=True)
     f = CACHE / f"scaled_ip_{n}.npz"
+    t0 = time.time()
     if f.exists():
         z = np.load(f)
         base, pool = z["base"], z["pool"]
     else:
         base = scaled_clusters(n, 96, 4096, seed=51, centers_seed=151)
         pool = scaled_clusters(50_000, 96, 4096, seed=52, centers_seed=151)
-        np.savez(f, base=base, pool=pool)
-    ix = cached_graph(v, f"scaled_ip_{n}", base, "ip", 24)
+        if n <= 2_000_000:
+            np.savez(f, base=base, pool=pool)
+    log(f"uneven: {n} x 96 data in {time.time() - t0:.1f} s")
+    build = {}
+    if n > 2_000_000:
+        # The large graph is built by this library's batched GPU build (the host build of 10M
+        # rows at M = 24 would take many minutes on the box's cores); not cached on disk.
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ix = v.HnswIndex(96, "ip", M=24, ef_construction=EF_CONSTRUCTION, seed=SEED)
+        ix.add(base, device=0)
+        torch.cuda.synchronize()
+        rep = ix.inspect()
+        build = {"builder": "gpu (HnswIndex.add(device=0))",
+                 "seconds": round(time.perf_counter() - t0, 1),
+                 "violations": rep["violations"], "reachable": rep["reachable"],
+                 "max_level": rep["max_level"], "graph_bytes": int(ix.info()["memory_bytes"])}
+        log(f"uneven: GPU build {build}")
+    else:
+        ix = cached_graph(v, f"scaled_ip_{n}", base, "ip", 24)
+        build = {"builder": "host parallel add (the reference's algorithm), cached"}
     ix.upload(0, "fp32")
     sizes, ks, efs = request_stream(5000, 51)
     offs = np.concatenate([[0], np.cumsum(sizes)])
@@ -753,14 +862,29 @@ def study_uneven(args, v, torch):
         if c is None or t["ms"] < c["ms"]:
             chosen[t["ef_class"]] = t
 
-    # Parity on every 50th request: the batcher's rows equal the plain search's.
+    # Parity on every 50th request: the batcher's rows equal the plain search's. Recall@10 of
+    # those requests with k >= 10 (their first 2,000 rows each) against exact brute force.
     mismatches = 0
+    judged = []
     for i in range(0, len(requests), 50):
         q, k, ef = requests[i]
         a, b, c = bt.run(q, k, ef)
         wa, wb, wc = ix.search_batch(q, k, ef)
         if not (np.array_equal(a[:, :k], wa) and np.array_equal(b[:, :k], wb) and np.array_equal(c, wc)):
             mismatches += 1
+        if k >= K:
+            judged.append((offs[i], min(len(q), 2000), a[:, :K]))
+    rows_judged = np.unique(np.concatenate([rows[o:o + m] for o, m, _ in judged]))
+    exact = v.BruteForceIndex(96, "ip")
+    exact.add(base)
+    t0 = time.time()
+    truth_rows, _, _ = exact.search_batch(pool[rows_judged], K)
+    log(f"uneven: exact truth of {len(rows_judged)} pool rows in {time.time() - t0:.1f} s")
+    del exact
+    where = {int(r): j for j, r in enumerate(rows_judged)}
+    found = np.concatenate([ids[:m] for _, m, ids in judged])
+    truth = np.stack([truth_rows[where[int(r)]] for o, m, _ in judged for r in rows[o:o + m]])
+    stream_recall = recall_at_10(found, truth)
 
     def serve(mode, depth=4, packs=None):
         lat = np.zeros(len(requests))
@@ -814,7 +938,13 @@ def study_uneven(args, v, torch):
             out[name] = serve("pipelined", depth, packs)
     line = {"study": "uneven", "workload": f"{n} x 96 IP, 4,096 clusters (log-normal scales), "
                                            f"M24 efc{EF_CONSTRUCTION}; 5,000 requests (seed 51)",
+            "graph": build,
             "queries": total_q, "batches_packed": len(batches), "modes": out,
+            "recall_at_10": {"value": round(stream_recall, 4), "queries": int(len(found)),
+                             "requests": len(judged),
+                             "judge": "exact brute force (this library's exact kernel, bit-identical "
+                                      "to the reference's BruteForceIndex) on the sampled requests "
+                                      "with k >= 10, their first 2,000 rows each"},
             "autotune_seconds": round(tune_s, 2),
             "plans": {str(k_): {f: c[f] for f in ("warps_per_block", "rows_per_round", "hash_slots",
                                                    "global_slots", "result_capacity", "ms")}
@@ -822,6 +952,87 @@ def study_uneven(args, v, torch):
             "parity_sampled_requests": len(range(0, len(requests), 50)),
             "parity_mismatches": mismatches, "clocks": clocks.summary()}
     print(json.dumps(line), flush=True)
+
+
+def study_learned(args, v, torch):
+    """Learned early termination as its configuration states it: the CPU-runnable graph
+    (10,000 x 128 L2, 100 isotropic clusters, M 16, ef_construction 200, the reference's serial
+    build), a model trained by this library's kernels on 200,000 training queries (seed 21) whose
+    labels come from plain ef = 512 traces judged by exact brute force, thresholds calibrated on
+    10,000 more queries (seed 23) for recall targets 0.95 / 0.97 / 0.99 at several ef caps, and
+    everything evaluated on 100,000 fresh queries (seed 22), FP32 traversal, k = 10, the network
+    consulted every 8 expansions with the ef cap as the fallback. For every learned operating
+    point: recall, layer-0 distance evaluations and device time, against the plain ef sweep at
+    equal recall (linear interpolation between the two sweep points around it)."""
+    from hnsw_vector_search_b200 import learned
+    from hnsw_vector_search_b200.datasets import integer_clusters
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as o
+    n_train, n_cal, n_eval = 200_000, 10_000, 100_000
+    base = integer_clusters(10_000, 128, 100, seed=1, centers_seed=101, sigma=12.0)
+    train_q = integer_clusters(n_train, 128, 100, seed=21, centers_seed=101, sigma=12.0)
+    eval_q = integer_clusters(n_eval, 128, 100, seed=22, centers_seed=101, sigma=12.0)
+    cal_q = integer_clusters(n_cal, 128, 100, seed=23, centers_seed=101, sigma=12.0)
+    CACHE.mkdir(exist_ok=True)
+    path = CACHE / "small_l2_M16_efc200_serial.vdx"
+    if not path.exists():
+        ref = o.RefHnsw(128, 0, M, EF_CONSTRUCTION, SEED)
+        ref.add(base, threads=1)
+        ref.save(path)
+        del ref
+    ix = v.HnswIndex.load(path)
+    bf = v.BruteForceIndex(128, "l2")
+    bf.add(base)
+    truth = {name: bf.search_batch(qs, K)[0] for name, qs in
+             (("train", train_q), ("cal", cal_q), ("eval", eval_q))}
+    t0 = time.time()
+    tr = learned.traces(ix, train_q, truth["train"], k=K, ef=512)
+    x, y = learned.training_set(tr)
+    model, losses = learned.train(x, y, tr["proj"], epochs=6)
+    train_s = time.time() - t0
+    dev = torch.device("cuda", 0)
+    eval_dev = torch.from_numpy(eval_q).to(dev)
+
+    plain = []
+    for ef in (10, 12, 14, 16, 20, 24, 28, 32, 40, 48, 64, 80, 96, 128, 192, 256, 384, 512):
+        ids, _, _ = ix.search_batch(eval_q, K, ef)
+        ms, st = device_ms(v, torch, ix, eval_dev, ef)
+        plain.append({"ef": ef, "recall": round(recall_at_10(ids, truth["eval"]), 5),
+                      "dist_layer0": st["dist_layer0"], "ms": round(ms, 4)})
+
+    def plain_at(rec, key):
+        pts = sorted(plain, key=lambda p: p["recall"])
+        for a, b in zip(pts, pts[1:]):
+            if a["recall"] <= rec <= b["recall"] and b["recall"] > a["recall"]:
+                w = (rec - a["recall"]) / (b["recall"] - a["recall"])
+                return a[key] + w * (b[key] - a[key])
+        return None
+
+    points = []
+    for cap in (64, 128, 256, 512):
+        for target in (0.95, 0.97, 0.99):
+            thr, rec_cal = learned.calibrate(ix, model, cal_q, truth["cal"], K, target, cap)
+            ids, _, _ = ix.search_batch(eval_q, K, cap, learned_stop=True, stop_threshold=thr)
+            rec = recall_at_10(ids, truth["eval"])
+            ms, st = device_ms(v, torch, ix, eval_dev, cap, learned_stop=True, stop_threshold=thr)
+            pd, pm = plain_at(rec, "dist_layer0"), plain_at(rec, "ms")
+            points.append({"ef_cap": cap, "target": target, "threshold": thr,
+                           "calibration_recall": round(rec_cal, 5), "recall": round(rec, 5),
+                           "dist_layer0": st["dist_layer0"], "stops": st["learned_stops"],
+                           "ms": round(ms, 4),
+                           "plain_dist_at_equal_recall": None if pd is None else int(pd),
+                           "plain_ms_at_equal_recall": None if pm is None else round(pm, 4),
+                           "evaluations_gain": None if pd is None else round(pd / st["dist_layer0"], 4),
+                           "time_gain": None if pm is None else round(pm / ms, 4)})
+    print(json.dumps({"study": "learned", "workload": "10,000 x 128 L2 (100 isotropic clusters, "
+                      "sigma 12), M16 efc200 serial reference build, k 10, FP32 traversal",
+                      "train_queries": n_train, "calibration_queries": n_cal,
+                      "eval_queries": n_eval, "labels": "plain ef 512 traces judged by exact brute "
+                      "force: a checkpoint is converged when its top-10 hits equal the final ones",
+                      "samples": int(len(x)), "positive_share": round(float(y.mean()), 4),
+                      "train_seconds_with_traces": round(train_s, 2),
+                      "loss_per_epoch": [round(float(l), 5) for l in losses],
+                      "plain": plain, "learned": points}), flush=True)
 
 
 def study_precision(args, v, torch):

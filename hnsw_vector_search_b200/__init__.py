@@ -51,7 +51,7 @@ class _GraphReport(ctypes.Structure):
 class SearchOptions(ctypes.Structure):
     """vdx_search_options: traversal precision, FP32 re-rank width, learned stop, device."""
     _fields_ = [("precision", _U32), ("rerank", _U32), ("learned_stop", _U32),
-                ("stop_threshold", _F), ("device", _I32)]
+                ("stop_threshold", _F), ("device", _I32), ("stop_gate", _U32)]
 
 
 _lib = None
@@ -152,11 +152,15 @@ def _rows(data, dim: int) -> np.ndarray:
     return a
 
 
-def _options(precision="fp32", rerank=0, learned_stop=False, stop_threshold=0.5, device=0):
-    """rerank: 0 = 4k candidates re-scored in FP32 (BF16 / FP8), "none" = no re-rank."""
+def _options(precision="fp32", rerank=0, learned_stop=False, stop_threshold=0.5, device=0,
+             stop_gate=0):
+    """rerank: 0 = 4k candidates re-scored in FP32 (BF16 / FP8), "none" = no re-rank.
+    stop_gate: the learned stop consults its network only once the k-th distance has been
+    unchanged for this many expansions in a row (0: at every checkpoint)."""
     rr = 0xFFFFFFFF if rerank == "none" else int(rerank)
     return SearchOptions(PRECISIONS[precision] if isinstance(precision, str) else int(precision),
-                         rr, 1 if learned_stop else 0, float(stop_threshold), int(device))
+                         rr, 1 if learned_stop else 0, float(stop_threshold), int(device),
+                         int(stop_gate))
 
 
 class HnswIndex:

@@ -72,6 +72,10 @@ vdx::SearchOptions options_of(const vdx_search_options* o) {
         s.rerank = o->rerank;
         s.learned_stop = o->learned_stop != 0;
         s.stop_threshold = o->stop_threshold;
+        if (o->stop_gate > 3) {
+            throw std::invalid_argument("stop_gate must be at most 3");
+        }
+        s.stop_gate = o->stop_gate;
         s.device = o->device;
     }
     return s;
@@ -332,6 +336,7 @@ vdx_status vdx_search_batch_device(const vdx_index* index, const float* d_querie
             a.stop = net.view;
             a.stop_enabled = &net;
             a.stop_threshold = o.stop_threshold;
+            a.stop_gate = o.stop_gate;
         }
         // Per-query ef: the capacity must cover the largest; the caller's uniform ef bounds it.
         const uint64_t cap = std::min<uint64_t>(std::max<uint64_t>(ef_uniform, kk), h.size());

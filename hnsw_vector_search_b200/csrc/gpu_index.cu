@@ -563,6 +563,7 @@ void HnswIndex::search_batch_into(MatrixView<float> queries, std::size_t k, std:
         a.stop = net.view;
         a.stop_enabled = &net;
         a.stop_threshold = options.stop_threshold;
+        a.stop_gate = options.stop_gate;
     }
     const std::size_t ef_eff = std::min<std::size_t>(std::max(ef, k), size());
     dev::SearchPlan plan = dev::default_plan(dg.view, static_cast<std::uint32_t>(ef_eff), true);

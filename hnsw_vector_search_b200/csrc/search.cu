@@ -122,9 +122,12 @@ __device__ __forceinline__ float sgnlog(float x) { return copysignf(log1pf(fabsf
 //   8..11 query projections
 // None depends on ef, so a model trained on traces at one ef cap reads the same features at
 // another. Called by every lane (the ballot of feature 7 needs the whole warp).
-__device__ __forceinline__ void stop_features(float* f, float qlen, float d_entry, const float* proj,
-                                              const float* rd, int r, int k, const float* hist,
-                                              int hops, int lane) {
+// `fc` holds the query's constant features: [0] |q|, [1] layer-0 entry distance, [2..5] the
+// projections.
+__device__ __forceinline__ void stop_features(float* f, const float* fc, const float* rd, int r,
+                                              int k, const float* hist, int hops, int lane) {
+    const float qlen = fc[0];
+    const float d_entry = fc[1];
     const int kk = r < k ? r : k;
     const float d1 = rd[0];
     const float dk = rd[kk - 1];
@@ -149,8 +152,18 @@ __device__ __forceinline__ void stop_features(float* f, float qlen, float d_entr
     f[7] = log1pf(static_cast<float>(unchanged > 0 ? unchanged : 0));
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-        f[8 + i] = proj[i];
+        f[8 + i] = fc[2 + i];
     }
+}
+
+// Expansions in a row, ending with the latest one, that left the k-th distance unchanged
+// (0 to 3): the stop's gate reads no more than that.
+__device__ __forceinline__ int recent_stagnation(const float* hist, int hops) {
+    const float a = hist[(hops - 1) & (kHist - 1)];
+    const float b = hist[(hops - 2) & (kHist - 1)];
+    const float c = hist[(hops - 3) & (kHist - 1)];
+    const float d = hist[(hops - 4) & (kHist - 1)];
+    return a != b ? 0 : (b != c ? 1 : (c != d ? 2 : 3));
 }
 
 // P(converged) of the network for features f (identical in every lane); h1 is 64 floats of
@@ -226,15 +239,21 @@ __device__ __forceinline__ float row_distance(const float* q, const unsigned cha
                       : pair_distance<P, kL2>(q, row, dim, row_bytes, half);
 }
 
+// Which learned-termination code a search kernel carries: none (plain searches), the stop only,
+// or the stop and the training traces.
+enum LearnMode : int { kLearnNone = 0, kLearnStop = 1, kLearnTrace = 2 };
+
 // kRegR: R in registers (RegBeam, result capacity up to 64) instead of shared memory.
-// kLearn: the learned stop and its training traces are compiled in (launched only when one of
-// them is on, so plain searches carry neither their code nor their registers; BF16 ef 36 7 %
-// faster). Without that code the compiler's own register target for the shared-memory-beam
-// kernels fell to 80 with spills, so those are bounded like the rest at 128 (2 blocks of 256).
+// kLearn: the learned-termination code compiled in (LearnMode; the variants launch only when the
+// stop or tracing is on, so plain searches carry neither the code nor its registers, BF16 ef 36
+// 7 % faster, and a stopping search does not carry the trace writer). Without that code the
+// compiler's own register target for the shared-memory-beam kernels fell to 80 with spills, so
+// those are bounded like the rest at 128 (2 blocks of 256).
 // kPass: the pass compiled (0 the whole search, 1 the descent of an ordered launch, 2 its layer-0
 // pass), so each kernel carries only the code its pass runs.
-template <int P, bool kL2, bool kRegR, bool kLearn, int kPass>
-__global__ void __launch_bounds__(kMaxThreads<P, kRegR>, kLowRegs<P, kRegR> ? 5 : (kLearn ? 0 : 2))
+template <int P, bool kL2, bool kRegR, int kLearn, int kPass>
+__global__ void __launch_bounds__(kMaxThreads<P, kRegR>,
+                                  kLowRegs<P, kRegR> ? 5 : (kLearn != kLearnNone ? 0 : 2))
     search_kernel(const SearchArgs a) {
     constexpr std::uint32_t pass = kPass;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -251,10 +270,11 @@ __global__ void __launch_bounds__(kMaxThreads<P, kRegR>, kLowRegs<P, kRegR> ? 5 
     int* ap = reinterpret_cast<int*>(ws + a.off_ap);
     float* hist = reinterpret_cast<float*>(ws + a.off_hist);  // kHist k-th distances
     float* h1 = hist + kHist;                                 // kHidden network scratch
+    float* fc = h1 + kHidden;                                 // the query's constant features
 
     const DeviceGraphView& g = a.g;
-    const bool learned = kLearn && a.stop_enabled != nullptr;
-    const bool tracing = kLearn && a.trace.truth != nullptr;
+    const bool learned = kLearn != kLearnNone && a.stop_enabled != nullptr;
+    const bool tracing = kLearn == kLearnTrace && a.trace.truth != nullptr;
     const auto* vecs = static_cast<const unsigned char*>(g.vectors);
     // A device-side batch size never exceeds the buffers' capacity (a.nq).
     const std::uint32_t nq = a.nq_device != nullptr ? min(*a.nq_device, a.nq) : a.nq;
@@ -361,17 +381,22 @@ __global__ void __launch_bounds__(kMaxThreads<P, kRegR>, kLowRegs<P, kRegR> ? 5 
         if (pass != 2) {
             ++c_q;
         }
-        float qlen = 0.0F;
-        float proj[4] = {0.0F, 0.0F, 0.0F, 0.0F};
         if ((learned || tracing) && pass != 1) {
-            qlen = sqrtf(warp_raw<kFP32, false>(q, reinterpret_cast<const unsigned char*>(q), g.dim,
-                                                g.row32 * 4, lane));
+            // The constant features go to shared memory: the walk keeps no registers for them.
+            const float qlen = sqrtf(warp_raw<kFP32, false>(
+                q, reinterpret_cast<const unsigned char*>(q), g.dim, g.row32 * 4, lane));
             const float inv = 1.0F / fmaxf(qlen, 1e-20F);
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
-                proj[i] = inv * warp_raw<kFP32, false>(
-                                    q, reinterpret_cast<const unsigned char*>(a.stop.proj + i * g.row32),
-                                    g.dim, g.row32 * 4, lane);
+                const float pr = inv * warp_raw<kFP32, false>(
+                                           q, reinterpret_cast<const unsigned char*>(a.stop.proj + i * g.row32),
+                                           g.dim, g.row32 * 4, lane);
+                if (lane == 0) {
+                    fc[2 + i] = pr;
+                }
+            }
+            if (lane == 0) {
+                fc[0] = qlen;
             }
         }
         std::uint32_t trace_points = 0;
@@ -509,7 +534,9 @@ __global__ void __launch_bounds__(kMaxThreads<P, kRegR>, kLowRegs<P, kRegR> ? 5 
         int scan = 0;
         int slot = 0;
         std::uint32_t prefetched = kNoId;
-        const float d_entry = curd;
+        if ((learned || tracing) && lane == 0) {
+            fc[1] = curd;  // the layer-0 entry distance
+        }
         int hops = 0;
         for (std::uint32_t step = 0; step <= g.n; ++step) {
             int p;
@@ -659,9 +686,13 @@ __global__ void __launch_bounds__(kMaxThreads<P, kRegR>, kLowRegs<P, kRegR> ? 5 
                     hist[(hops - 1) & (kHist - 1)] = rd[kk - 1];
                 }
                 __syncwarp();
-                if ((hops & 7) == 0) {
+                // Every 8 expansions: traces record the state; the stop consults the network
+                // once the k-th distance has been unchanged for stop_gate expansions in a row
+                // (0: at every checkpoint). While it still improves, the beam is not done.
+                if ((hops & 7) == 0 &&
+                    (tracing || static_cast<std::uint32_t>(recent_stagnation(hist, hops)) >= a.stop_gate)) {
                     float f[kFeatures];
-                    stop_features(f, qlen, d_entry, proj, rd, r, static_cast<int>(k), hist, hops, lane);
+                    stop_features(f, fc, rd, r, static_cast<int>(k), hist, hops, lane);
                     if (tracing && trace_points < a.trace.max_points) {
                         const std::size_t at = static_cast<std::size_t>(qi) * a.trace.max_points + trace_points;
                         if (lane < kFeatures) {
@@ -915,9 +946,17 @@ cudaError_t resident_blocks(const void* kernel, int device, int threads, std::si
 // tracing is on).
 template <int P, bool kL2, bool kRegR, int kPass>
 const void* pass_kernel(const SearchArgs& args) {
-    const bool learn = args.stop_enabled != nullptr || args.trace.truth != nullptr;
-    return learn ? reinterpret_cast<const void*>(&search_kernel<P, kL2, kRegR, true, kPass>)
-                 : reinterpret_cast<const void*>(&search_kernel<P, kL2, kRegR, false, kPass>);
+    if constexpr (kPass == 1) {
+        return reinterpret_cast<const void*>(&search_kernel<P, kL2, kRegR, kLearnNone, 1>);  // no stop
+    } else {
+        if (args.trace.truth != nullptr) {
+            return reinterpret_cast<const void*>(&search_kernel<P, kL2, kRegR, kLearnTrace, kPass>);
+        }
+        if (args.stop_enabled != nullptr) {
+            return reinterpret_cast<const void*>(&search_kernel<P, kL2, kRegR, kLearnStop, kPass>);
+        }
+        return reinterpret_cast<const void*>(&search_kernel<P, kL2, kRegR, kLearnNone, kPass>);
+    }
 }
 
 template <int P, bool kL2, bool kRegR>
@@ -1074,7 +1113,7 @@ std::size_t plan_search(SearchArgs& a, const SearchPlan& plan) {
     if (a.stop_enabled != nullptr || a.trace.truth != nullptr) {
         // Only the learned stop and its traces read the history ring and network scratch; the
         // kernel takes both flags from these same arguments, so the layout always matches.
-        off += (kHist + kHidden) * 4;
+        off += (kHist + kHidden + 8) * 4;
     }
     a.warp_bytes = round_up(off, 16);
     return static_cast<std::size_t>(a.warp_bytes) * plan.warps_per_block;

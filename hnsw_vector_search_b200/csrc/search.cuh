@@ -90,6 +90,9 @@ struct SearchArgs {
     std::uint32_t gwarps = 0;               // warps the tables were sized for
     float stop_threshold = 0.5F;
     std::uint32_t stop_min_hops = 16;
+    // The network is consulted at a checkpoint only when the k-th distance has been unchanged
+    // for this many expansions in a row (0 to 3; 0 consults it at every checkpoint).
+    std::uint32_t stop_gate = 0;
     TraceArgs trace{};
     // Ordered launch (all three non-null, nq words each): a descent pass writes each query's
     // layer-0 entry (id, distance; id 0xFFFFFFFF for a query that failed its checks), the queries

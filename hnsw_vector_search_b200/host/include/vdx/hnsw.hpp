@@ -74,6 +74,9 @@ struct SearchOptions {
     // (HnswIndex::set_stop_model); ef stays the hard cap.
     bool learned_stop = false;
     float stop_threshold = 0.5F;
+    // Consult the network only once the k-th distance has been unchanged for this many
+    // expansions in a row (0 to 3; 0: at every checkpoint).
+    std::uint32_t stop_gate = 0;
     int device = 0;
 };
 

@@ -30,7 +30,7 @@ from .recall import recall_at_k
 
 FEATURES = 12
 PARAMS = 5057
-MODEL_VERSION = 2
+MODEL_VERSION = 3
 
 
 def _bind():
@@ -61,10 +61,12 @@ class StopModel:
     proj: np.ndarray      # [4, dim]
     threshold: float = 0.5
     ef_cap: int = 128
+    gate: int = 0         # consult the network only after this many unchanged expansions
 
     def save(self, path) -> None:
         np.savez(path, version=MODEL_VERSION, weights=self.weights, mean=self.mean,
-                 inv_std=self.inv_std, proj=self.proj, threshold=self.threshold, ef_cap=self.ef_cap)
+                 inv_std=self.inv_std, proj=self.proj, threshold=self.threshold, ef_cap=self.ef_cap,
+                 gate=self.gate)
 
     @classmethod
     def load(cls, path) -> "StopModel":
@@ -73,7 +75,7 @@ class StopModel:
             raise ValueError(f"{path}: stop model version {int(z['version'])} is not supported")
         return cls(z["weights"].astype(np.float32), z["mean"].astype(np.float32),
                    z["inv_std"].astype(np.float32), z["proj"].astype(np.float32),
-                   float(z["threshold"]), int(z["ef_cap"]))
+                   float(z["threshold"]), int(z["ef_cap"]), int(z["gate"]))
 
 
 def random_projections(dim: int, seed: int = 404) -> np.ndarray:
@@ -179,4 +181,5 @@ def calibrate(index, model: StopModel, queries: np.ndarray, truth: np.ndarray, k
             break
         best = (t, r)
     model.threshold, model.ef_cap = best[0], ef_cap
+    model.gate = int(options.get("stop_gate", 0))
     return best

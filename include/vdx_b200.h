@@ -67,6 +67,9 @@ typedef struct vdx_search_options {
     uint32_t learned_stop;   /* nonzero: learned early termination (needs a model) */
     float stop_threshold;    /* stop when the network's "converged" probability reaches this */
     int32_t device;
+    uint32_t stop_gate;      /* learned stop: consult the network at a checkpoint only once the k-th
+                                distance has been unchanged for this many expansions in a row
+                                (0 to 3; 0 = at every checkpoint) */
 } vdx_search_options;
 
 /* Statistics words of a search (vdx_last_stats, vdx_search_batch_device). */

@@ -228,6 +228,11 @@ class Oracle:
             L.vo_index_size.argtypes = [_P]
             L.vo_index_dim.restype = _U64
             L.vo_index_dim.argtypes = [_P]
+            for n in ("vo_bf16_round", "vo_e4m3_round"):
+                getattr(L, n).restype = _F
+                getattr(L, n).argtypes = [_F]
+            L.vo_quantize_rows.argtypes = [ctypes.c_int, _P, _U64, _U64, _P]
+            L.vo_index_quantize.argtypes = [_P, ctypes.c_int]
             Oracle._lib = L
         self.L = Oracle._lib
 
@@ -240,6 +245,15 @@ class Oracle:
         a = np.ascontiguousarray(a, np.float32)
         b = np.ascontiguousarray(b, np.float32)
         return float(self.L.vo_ip(_p(a), _p(b), a.size))
+
+    def quantize_rows(self, rows, precision: str) -> np.ndarray:
+        """The GPU traversal copy of `rows` as FP32 values: "bf16" (round to nearest even) or
+        "fp8" (E4M3 with a per-row FP32 scale max|x| / 448, round to nearest even, saturating)."""
+        a = np.ascontiguousarray(rows, np.float32)
+        out = np.empty_like(a)
+        code = {"fp32": 0, "bf16": 1, "fp8": 2}[precision]
+        self.L.vo_quantize_rows(code, _p(a), a.shape[0], a.shape[1], _p(out))
+        return out
 
     def integer_matrix(self, rows, dim, seed) -> np.ndarray:
         out = np.empty((rows, dim), np.float32)
@@ -278,6 +292,11 @@ class OracleIndex:
         if getattr(self, "h", None):
             self.o.L.vo_index_free(self.h)
             self.h = None
+
+    def quantize(self, precision: str) -> None:
+        """Replaces the stored vectors by their traversal copy ("bf16" or "fp8"), so that
+        searches run the GPU's low-precision traversal."""
+        self.o.L.vo_index_quantize(self.h, {"bf16": 1, "fp8": 2}[precision])
 
     def search_batch(self, queries, k, ef, stats=False):
         q = np.ascontiguousarray(queries, np.float32)

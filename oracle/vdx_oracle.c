@@ -262,6 +262,69 @@ static const uint32_t* links(const vo_index* ix, uint64_t node, uint64_t layer) 
 static const float* vec(const vo_index* ix, uint64_t id) { return ix->vectors + id * ix->dim; }
 
 /* ------------------------------------------------------------------------------------------ */
+/* Traversal copies of the stored vectors (no reference counterpart: the reference searches     */
+/* FP32 only). What the GPU traversal reads, as the FP32 values it computes with:               */
+/*   BF16: every element rounded to bfloat16, round to nearest, ties to even;                   */
+/*   FP8:  one FP32 scale per row, s = max|x| / 448 (1 when the row is zero), every element     */
+/*         x / s rounded to E4M3 (1-4-3, bias 7, max finite 448, subnormal quantum 2^-9),       */
+/*         round to nearest, ties to even, saturating at +-448, then read back as s * e4m3.     */
+/* Distances then follow the reference's kernel order on these values (FP32 accumulation).     */
+/* ------------------------------------------------------------------------------------------ */
+
+float vo_bf16_round(float x) {
+    uint32_t u;
+    memcpy(&u, &x, 4);
+    u += 0x7FFFu + ((u >> 16) & 1u); /* half of the dropped range, plus one on an odd kept lsb */
+    u &= 0xFFFF0000u;
+    float r;
+    memcpy(&r, &u, 4);
+    return r;
+}
+
+float vo_e4m3_round(float v) {
+    const float a = fabsf(v);
+    float r;
+    if (a >= 448.0F) {
+        r = 448.0F;
+    } else {
+        int e2;
+        (void)frexpf(a, &e2);                         /* a = f * 2^e2, f in [0.5, 1) */
+        const int e = a >= 0x1p-6F ? e2 - 1 : -6;     /* binade exponent; subnormals share 2^-6 */
+        const float quantum = ldexpf(1.0F, e - 3);    /* 3 mantissa bits */
+        r = rintf(a / quantum) * quantum;             /* exact scaling; rintf rounds half to even */
+    }
+    return copysignf(r, v); /* E4M3 keeps the sign of zero too */
+}
+
+void vo_quantize_rows(int precision, const float* in, uint64_t n, uint64_t dim, float* out) {
+    for (uint64_t i = 0; i < n; ++i) {
+        const float* x = in + i * dim;
+        float* y = out + i * dim;
+        if (precision == 1) {
+            for (uint64_t e = 0; e < dim; ++e) {
+                y[e] = vo_bf16_round(x[e]);
+            }
+        } else if (precision == 2) {
+            float m = 0.0F;
+            for (uint64_t e = 0; e < dim; ++e) {
+                m = fmaxf(m, fabsf(x[e]));
+            }
+            const float s = m > 0.0F ? m / 448.0F : 1.0F;
+            for (uint64_t e = 0; e < dim; ++e) {
+                y[e] = s * vo_e4m3_round(x[e] / s);
+            }
+        } else {
+            memcpy(y, x, dim * 4);
+        }
+    }
+}
+
+/* Replaces a loaded index's vectors by their traversal copy (precision 1 BF16, 2 FP8). */
+void vo_index_quantize(vo_index* ix, int precision) {
+    vo_quantize_rows(precision, ix->vectors, ix->n, ix->dim, ix->vectors);
+}
+
+/* ------------------------------------------------------------------------------------------ */
 /* Search: src/hnsw.cpp:416-522.                                                              */
 /* ------------------------------------------------------------------------------------------ */
 

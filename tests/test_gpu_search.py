@@ -260,19 +260,55 @@ def test_fp8_traversal_with_rerank_keeps_recall(gpu, orc, small_l2):
             assert np.float32(o.l2(queries[q], base[ids8[q, i]])) == d8[q, i]
 
 
-def test_low_precision_without_rerank_returns_traversal_distances(gpu, orc, small_l2):
-    """rerank="none": the returned distances are the traversal-precision ones (FP8 rows, FP32
-    accumulation), within the E4M3 quantization error of the exact distances, and sorted."""
-    path, base, queries = small_l2
-    ix = gpu.HnswIndex.load(path)
-    ids, d, c = ix.search_batch(queries, 10, 64, precision="fp8", rerank="none")
-    ids_rr, d_rr, _ = ix.search_batch(queries, 10, 64, precision="fp8")
-    assert np.all(np.diff(d, axis=1) >= 0)
-    exact = np.array([[np.sum((queries[q].astype(np.float64) - base[i]) ** 2) for i in ids[q]]
-                      for q in range(len(queries))])
-    # E4M3 keeps 3 mantissa bits: each stored component is off by at most 1/16 of itself.
-    assert np.all(np.abs(d - exact) <= 0.25 * exact + 1.0)
-    assert not np.array_equal(d, d_rr)  # the default re-rank really re-scores in FP32
+def _stored_rows(orc, base, metric):
+    """The rows as the index stores them: normalized in the reference's order under cosine."""
+    rows = np.array(base, np.float32, copy=True)
+    if metric == 2:
+        for r in rows:
+            orc.Oracle().L.vo_normalize(r.ctypes.data, r.size)
+    return rows
+
+
+def _exact(orc, metric, q, row):
+    o = orc.Oracle()
+    return np.float32(o.l2(q, row)) if metric == 0 else np.float32(1.0) - np.float32(o.ip(q, row))
+
+
+@pytest.mark.parametrize("precision", ["bf16", "fp8"])
+@pytest.mark.parametrize("metric", [0, 1, 2])
+def test_low_precision_traversal_equals_the_quantized_oracle(gpu, orc, tmp_path, precision, metric):
+    """BF16 / FP8 traversal on real-valued data, bit for bit. The oracle quantizes the stored
+    rows as the GPU does (round to nearest even; E4M3 with the per-row FP32 scale max|x| / 448)
+    and runs the reference's search on them: with rerank="none" the GPU returns exactly those ids
+    and distances. With a re-rank of r, the GPU's result is the oracle's best min(r, ef)
+    candidates re-scored with the exact FP32 distance in the reference's order, best k by
+    (distance, id)."""
+    dim = 40
+    base = uniform_matrix(2000, dim, 11)
+    queries = uniform_matrix(120, dim, 12)
+    ref = orc.RefHnsw(dim, metric, 8, 60, 42)
+    ref.add(base, threads=0)
+    ref.save(tmp_path / "g.vdx")
+    ix = gpu.HnswIndex.load(tmp_path / "g.vdx")
+    quant = orc.OracleIndex(tmp_path / "g.vdx")
+    quant.quantize(precision)
+    stored = _stored_rows(orc, base, metric)
+    for k, ef in [(1, 1), (10, 10), (10, 40), (10, 150)]:
+        got = ix.search_batch(queries, k, ef, precision=precision, rerank="none")
+        want = quant.search_batch(queries, k, ef)
+        assert_same(got, want[:3], f"{precision} metric {metric} k {k} ef {ef}")
+    k, ef, r = 10, 64, 24
+    ids, d, c = ix.search_batch(queries, k, ef, precision=precision, rerank=r)
+    cand, _, cc = quant.search_batch(queries, min(r, ef), ef)[:3]
+    for qi in range(len(queries)):
+        q = np.array(queries[qi], np.float32, copy=True)
+        if metric == 2:
+            orc.Oracle().L.vo_normalize(q.ctypes.data, q.size)
+        scored = sorted((_exact(orc, metric, q, stored[i]), int(i)) for i in cand[qi, :cc[qi]])[:k]
+        assert c[qi] == len(scored)
+        assert [i for _, i in scored] == ids[qi, :c[qi]].tolist(), f"query {qi}"
+        assert np.array([x for x, _ in scored], np.float32).view(np.uint32).tolist() == \
+            d[qi, :c[qi]].view(np.uint32).tolist(), f"query {qi}"
 
 
 def test_device_api_with_per_query_k_and_ef(gpu, small_l2):

@@ -137,3 +137,33 @@ def test_distance_known_values(orc):
     assert o.l2(a, b) == float(((a - b).astype(np.int64) ** 2).sum())
     assert o.ip(np.array([1.0, 2, 3]), np.array([4.0, -5, 6])) == 12.0
     assert o.l2(np.zeros(0), np.zeros(0)) == 0.0
+
+
+def test_traversal_quantizers_match_torch(orc):
+    """The oracle's BF16 and E4M3 rounding (which pins the GPU's low-precision traversal) against
+    torch's independent CPU conversions, on values spread over 2^-30 .. 2^10 with subnormal E4M3
+    inputs, exact ties, +-0 and the saturation edge (torch's E4M3 cast does not saturate, so its
+    inputs are clipped to +-448 first)."""
+    torch = pytest.importorskip("torch")
+    o = orc.Oracle()
+    rng = np.random.default_rng(0)
+    x = (rng.standard_normal(20000) * np.exp(rng.uniform(-20, 7, 20000))).astype(np.float32)
+    edge = np.array([0.0, -0.0, 448, -448, 447.9, 464, 500, -1e9, 2 ** -9, 2 ** -10, 3 * 2 ** -11,
+                     1.0625, 1.1875, -1.0625, 2 ** -6 * 1.0625, 2 ** -6 * 1.1875, 3 * 2 ** -10],
+                    np.float32)
+    x = np.concatenate([x, edge])
+    e4m3 = np.array([o.L.vo_e4m3_round(float(v)) for v in x], np.float32)
+    want = torch.from_numpy(np.clip(x, -448, 448)).to(torch.float8_e4m3fn).to(torch.float32).numpy()
+    np.testing.assert_array_equal(e4m3.view(np.uint32), want.view(np.uint32))
+    bf = np.array([o.L.vo_bf16_round(float(v)) for v in x], np.float32)
+    want = torch.from_numpy(x).to(torch.bfloat16).to(torch.float32).numpy()
+    np.testing.assert_array_equal(bf.view(np.uint32), want.view(np.uint32))
+    # Whole rows: FP8 with the per-row scale max|x| / 448 (the largest element maps to 448).
+    rows = rng.uniform(-3, 3, size=(50, 37)).astype(np.float32)
+    q8 = o.quantize_rows(rows, "fp8")
+    s = (np.abs(rows).max(axis=1) / np.float32(448)).astype(np.float32)
+    codes = torch.from_numpy(np.clip(rows / s[:, None], -448, 448)).to(torch.float8_e4m3fn)
+    back = (s[:, None] * codes.to(torch.float32).numpy()).astype(np.float32)
+    np.testing.assert_array_equal(q8.view(np.uint32), back.view(np.uint32))
+    np.testing.assert_array_equal(o.quantize_rows(rows, "bf16").view(np.uint32),
+                                  torch.from_numpy(rows).to(torch.bfloat16).to(torch.float32).numpy().view(np.uint32))
