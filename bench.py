@@ -280,7 +280,8 @@ def main():
     ap.add_argument("--impl", default="vdx")
     ap.add_argument("--profile", action="store_true",
                     help="one search launch per warm-up step on the cached workload (for ncu)")
-    ap.add_argument("--mode", default="fp32", choices=["fp32", "bf16", "fp8", "bf_tc", "bf_exact"])
+    ap.add_argument("--mode", default="fp32",
+                    choices=["fp32", "bf16", "fp8", "bf_tc", "bf_exact", "mlp", "build"])
     ap.add_argument("--ef", type=int, default=32)
     ap.add_argument("--study", choices=["uneven", "precision", "build", "device_image", "learned"],
                     help="instead of the headline: the uneven-batch stream or the precision study")
@@ -885,6 +886,14 @@ def study_uneven(args, v, torch):
     found = np.concatenate([ids[:m] for _, m, ids in judged])
     truth = np.stack([truth_rows[where[int(r)]] for o, m, _ in judged for r in rows[o:o + m]])
     stream_recall = recall_at_10(found, truth)
+    # The graph's own ceiling: recall@10 of the plain search of 2,000 pool queries per ef.
+    probe = pool[:2000]
+    exact = v.BruteForceIndex(96, "ip")
+    exact.add(base)
+    probe_truth, _, _ = exact.search_batch(probe, K)
+    del exact
+    recall_by_ef = {ef: round(recall_at_10(ix.search_batch(probe, K, ef)[0], probe_truth), 4)
+                    for ef in (10, 32, 64, 128, 256, 512, 656)}
 
     def serve(mode, depth=4, packs=None):
         lat = np.zeros(len(requests))
@@ -940,6 +949,7 @@ def study_uneven(args, v, torch):
                                            f"M24 efc{EF_CONSTRUCTION}; 5,000 requests (seed 51)",
             "graph": build,
             "queries": total_q, "batches_packed": len(batches), "modes": out,
+            "recall_at_10_by_ef": recall_by_ef,
             "recall_at_10": {"value": round(stream_recall, 4), "queries": int(len(found)),
                              "requests": len(judged),
                              "judge": "exact brute force (this library's exact kernel, bit-identical "
@@ -1157,11 +1167,30 @@ def study_device_image(args, v, torch):
 
 def profile(args, v, torch):
     """`warmup` + 1 launches of the search kernel on the cached 1M workload, nothing else on
-    the GPU in between: the command the committed ncu summaries were captured from."""
+    the GPU in between: the command the committed ncu summaries were captured from. Other
+    modes: `bf_tc` / `bf_exact` the brute-force pipelines on the same data; `mlp` one epoch of
+    the learned stop's training kernels (forward, backward, Adam) on 262,144 synthetic samples,
+    then the batched probabilities; `build` the GPU graph build of 200,000 rows of the same
+    data (M 16, ef_construction 200)."""
+    if args.mode == "mlp":
+        from hnsw_vector_search_b200 import learned
+        g = np.random.default_rng(5)
+        x = g.standard_normal((262_144, learned.FEATURES)).astype(np.float32)
+        y = (x[:, 0] + 0.5 * x[:, 7] > 0).astype(np.float32)
+        model, losses = learned.train(x, y, learned.random_projections(128), epochs=1)
+        p = learned.probabilities(model, x[:65536])
+        print(json.dumps({"profile": "mlp", "loss": float(losses[-1]), "p_mean": float(p.mean())}))
+        return
     base, queries = workload()
+    if args.mode == "build":
+        ix = v.HnswIndex(128, "l2", M=M, ef_construction=EF_CONSTRUCTION, seed=SEED)
+        ix.add(base[:200_000], device=0)
+        torch.cuda.synchronize()
+        print(json.dumps({"profile": "build", "violations": ix.inspect()["violations"]}))
+        return
     if args.mode.startswith("bf_"):
         bf = v.BruteForceIndex(base.shape[1], "l2")
-        bf.add(base)
+        bf.add(base[:args.rows] if args.rows else base)  # --rows: a smaller base for a capture
         dev = torch.device("cuda", 0)
         q = torch.from_numpy(queries).to(dev)
         nq = len(queries)

@@ -106,6 +106,7 @@ def lib() -> ctypes.CDLL:
         "vdx_host_l2": (_F, [_P, _P, _U64]),
         "vdx_host_ip": (_F, [_P, _P, _U64]),
         "vdx_xxh64": (_U64, [_P, _U64, _U64]),
+        "vdx_testing_set_tc_wait_ns": (None, [_U64]),
         "vdx_search_kernels_last": (_U32, []),
     }
     for name, (res, args) in sigs.items():

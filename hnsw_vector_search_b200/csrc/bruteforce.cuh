@@ -56,5 +56,9 @@ std::size_t bruteforce_tc_workspace(std::uint32_t nq, std::uint32_t n, std::uint
                                     std::uint32_t k);
 cudaError_t launch_bruteforce_tc(const BruteArgs& args, const TcBase& base, void* workspace,
                                  cudaStream_t stream, std::uint32_t* uncertified_out);
+// The limit of each pipeline wait of the next tensor-core launches, in nanoseconds (0 restores
+// the default, 1 s). For tests of the timeout path; the drains before a CTA exits keep 1 s.
+std::uint64_t tc_wait_ns();
+void set_tc_wait_ns(std::uint64_t ns);
 
 }  // namespace vdx::dev

@@ -27,6 +27,7 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <cstring>
 #include <mutex>
@@ -73,10 +74,11 @@ __device__ __forceinline__ bool mbar_try(std::uint32_t a, std::uint32_t parity) 
         : "memory");
     return ok != 0;
 }
-// Waits for the phase with `parity` to complete; false after kWaitNs or once another role has
-// aborted.
+// Waits for the phase with `parity` to complete; false after `limit_ns` or once another role
+// has aborted. The pipeline's waits use the launch's limit (kWaitNs unless a test shortens it);
+// the drains before the CTA exits always use the full kWaitNs.
 __device__ __forceinline__ bool mbar_wait(std::uint32_t a, std::uint32_t parity,
-                                          volatile std::uint32_t* abort_flag) {
+                                          volatile std::uint32_t* abort_flag, std::uint64_t limit_ns) {
     if (mbar_try(a, parity)) {
         return true;
     }
@@ -85,10 +87,20 @@ __device__ __forceinline__ bool mbar_wait(std::uint32_t a, std::uint32_t parity,
         if (mbar_try(a, parity)) {
             return true;
         }
-        if (*abort_flag != 0 || now_ns() - t0 > kWaitNs) {
+        if (*abort_flag != 0 || now_ns() - t0 > limit_ns) {
             return false;
         }
     }
+}
+// Bounded by the full kWaitNs, for the drains: true when the phase completed.
+__device__ __forceinline__ bool mbar_drain(std::uint32_t a, std::uint32_t parity) {
+    const std::uint64_t t0 = now_ns();
+    while (!mbar_try(a, parity)) {
+        if (now_ns() - t0 > kWaitNs) {
+            return false;
+        }
+    }
+    return true;
 }
 __device__ __forceinline__ void tma_load_2d(std::uint32_t dst, const CUtensorMap* map, int x,
                                             int y, std::uint32_t mbar) {
@@ -188,6 +200,7 @@ struct TcParams {
     float* cand_tau;                      // [nq][nchunks * halves]
     std::uint32_t* floor_key;             // [nq] best kc-th score of any finished chunk (ordered key)
     std::uint32_t* error;                 // status word: 5 on a timeout
+    std::uint64_t wait_ns;                // limit of each pipeline wait (the drains keep kWaitNs)
     std::uint32_t off_b, off_lists, off_bar;  // smem offsets from the 1024-aligned base
 };
 
@@ -255,12 +268,12 @@ __global__ void __launch_bounds__(kThreads, 1)
 
     if (warp == 0 && lane == 0) {
         // TMA producer.
-        std::uint32_t it = 0, item_idx = 0;
+        std::uint32_t it = 0, item_idx = 0, a_loads = 0;
         bool ok = true;
         for (std::uint32_t item = blockIdx.x; ok && item < items; item += gridDim.x, ++item_idx) {
             const std::uint32_t qt = item % p.qtiles;
             const std::uint32_t ch = item / p.qtiles;
-            if (item_idx > 0 && !mbar_wait(a_empty, (item_idx - 1) & 1u, abort_flag)) {
+            if (item_idx > 0 && !mbar_wait(a_empty, (item_idx - 1) & 1u, abort_flag, p.wait_ns)) {
                 fail();
                 ok = false;
                 break;
@@ -274,13 +287,14 @@ __global__ void __launch_bounds__(kThreads, 1)
                                 static_cast<int>(qt * kBM), a_full);
                 }
             }
+            ++a_loads;
             const std::uint32_t row0 = ch * p.chunk_rows;
             const std::uint32_t rows = min(p.chunk_rows, p.n - row0);
             const std::uint32_t tiles = (rows + kBN - 1) / kBN;
             for (std::uint32_t t = 0; t < tiles; ++t, ++it) {
                 const std::uint32_t s = it % S;
                 const std::uint32_t ph = (it / S) & 1u;
-                if (!mbar_wait(empty(s), ph ^ 1u, abort_flag)) {
+                if (!mbar_wait(empty(s), ph ^ 1u, abort_flag, p.wait_ns)) {
                     fail();
                     ok = false;
                     break;
@@ -297,14 +311,17 @@ __global__ void __launch_bounds__(kThreads, 1)
                 }
             }
         }
-        if (!ok) {
-            // Let every copy this thread issued land before the CTA exits (bounded): the loads
-            // of the last min(S, it) tiles, tile i on stage i % S with phase parity (i / S) & 1.
-            for (std::uint32_t i = it > S ? it - S : 0; i < it; ++i) {
-                const std::uint64_t t0 = now_ns();
-                while (!mbar_try(full(i % S), (i / S) & 1u) && now_ns() - t0 < kWaitNs) {
-                }
-            }
+        // Every copy this thread issued lands before the CTA exits, whichever role stopped the
+        // pipeline (bounded by the full kWaitNs): the loads of the last min(S, it) tiles, tile i
+        // on stage i % S with phase parity (i / S) & 1, and the last query tile (phase
+        // a_loads - 1 of a_full). On the normal path these phases are long complete and the
+        // waits return at once.
+        (void)ok;
+        for (std::uint32_t i = it > S ? it - S : 0; i < it; ++i) {
+            mbar_drain(full(i % S), (i / S) & 1u);
+        }
+        if (a_loads > 0) {
+            mbar_drain(a_full, (a_loads - 1) & 1u);
         }
     } else if (warp == 1 && lane == 0) {
         // MMA issuer.
@@ -315,7 +332,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             const std::uint32_t row0 = ch * p.chunk_rows;
             const std::uint32_t rows = min(p.chunk_rows, p.n - row0);
             const std::uint32_t tiles = (rows + kBN - 1) / kBN;
-            if (!mbar_wait(a_full, item_idx & 1u, abort_flag)) {
+            if (!mbar_wait(a_full, item_idx & 1u, abort_flag, p.wait_ns)) {
                 fail();
                 ok = false;
                 break;
@@ -324,8 +341,8 @@ __global__ void __launch_bounds__(kThreads, 1)
             for (std::uint32_t t = 0; t < tiles; ++t, ++it, ++acc_it) {
                 const std::uint32_t s = it % S;
                 const std::uint32_t b = acc_it & 1u;
-                if (!mbar_wait(tempty0 + 8 * b, ((acc_it >> 1) & 1u) ^ 1u, abort_flag) ||
-                    !mbar_wait(full(s), (it / S) & 1u, abort_flag)) {
+                if (!mbar_wait(tempty0 + 8 * b, ((acc_it >> 1) & 1u) ^ 1u, abort_flag, p.wait_ns) ||
+                    !mbar_wait(full(s), (it / S) & 1u, abort_flag, p.wait_ns)) {
                     fail();
                     ok = false;
                     break;
@@ -356,9 +373,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         // Every MMA this thread issued has completed before TMEM is freed (bounded).
         mma_commit(drain);
-        const std::uint64_t t0 = now_ns();
-        while (!mbar_try(drain, 0) && now_ns() - t0 < kWaitNs) {
-        }
+        mbar_drain(drain, 0);
     } else if (warp >= 4 && static_cast<std::uint32_t>(warp - 4) < 4 * p.halves) {
         // Epilogue: thread e owns query row e of the tile (TMEM lane e) in column half `half`
         // of every tile (with halves = 2, two warps per TMEM lane quarter split the 128 columns,
@@ -396,7 +411,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             bool ok = true;
             for (std::uint32_t t = 0; t < tiles; ++t, ++acc_it) {
                 const std::uint32_t b = acc_it & 1u;
-                if (!mbar_wait(tfull0 + 8 * b, (acc_it >> 1) & 1u, abort_flag)) {
+                if (!mbar_wait(tfull0 + 8 * b, (acc_it >> 1) & 1u, abort_flag, p.wait_ns)) {
                     fail();
                     ok = false;
                     break;
@@ -776,6 +791,9 @@ bool make_map(CUtensorMap* map, const void* ptr, std::uint32_t rows, std::uint32
 
 std::size_t align_up(std::size_t x, std::size_t a) { return (x + a - 1) / a * a; }
 
+// The pipeline-wait limit of the next launches (nanoseconds; kWaitNs unless a test set it).
+std::atomic<std::uint64_t> g_tc_wait_ns{kWaitNs};
+
 struct Plan {
     std::uint32_t dk, kchunks, kc, stages, qtiles, nchunks, chunk_rows, halves;
     std::uint32_t off_b, off_lists, off_bar;
@@ -829,6 +847,9 @@ Plan make_plan(std::uint32_t nq, std::uint32_t n, std::uint32_t dim, std::uint32
 }
 
 }  // namespace
+
+std::uint64_t tc_wait_ns() { return g_tc_wait_ns.load(); }
+void set_tc_wait_ns(std::uint64_t ns) { g_tc_wait_ns.store(ns == 0 ? kWaitNs : ns); }
 
 struct TcBase {
     void* hi = nullptr;
@@ -915,7 +936,10 @@ std::size_t bruteforce_tc_workspace(std::uint32_t nq, std::uint32_t n, std::uint
     cudaGetDevice(&device);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     const Plan pl = make_plan(nq, n, dim, k, true, sms);
-    const std::size_t chunks = pl.ok ? static_cast<std::size_t>(pl.nchunks) * pl.halves : 1;
+    // Candidate lists per query: chunks x column halves. The launch's plan may use two halves
+    // where this one (sized for the largest stage) uses one, and the chunk count depends only on
+    // the shapes, so size for two.
+    const std::size_t chunks = pl.ok ? static_cast<std::size_t>(pl.nchunks) * 2 : 1;
     const std::size_t kc = pl.ok ? pl.kc : 32;
     return 4 * nqp * dk                         // q hi + lo
            + 4 * nqp * row32                    // normalized FP32 queries
@@ -1014,6 +1038,7 @@ cudaError_t launch_bruteforce_tc(const BruteArgs& a, const TcBase& b, void* work
     p.cand_tau = cand_tau;
     p.floor_key = floor_key;
     p.error = a.status;
+    p.wait_ns = tc_wait_ns();
     p.off_b = pl.off_b;
     p.off_lists = pl.off_lists;
     p.off_bar = pl.off_bar;

@@ -684,9 +684,11 @@ void HnswIndex::add_gpu(MatrixView<float> vectors, int device) {
     }
     entry_point_ = entry;
     max_level_ = max_level;
-    // The FP32 device mirror was built in place; its entry and top layer are now the host's.
+    // The FP32 device mirror was built in place; its entry and top layer are now the host's,
+    // and its upper copy is made from the finished upper layers.
     dg.view.entry = entry_point_;
     dg.view.max_level = static_cast<std::uint32_t>(max_level_);
+    gpu::attach_upper_copy(*this, dg, stream);
 }
 
 }  // namespace vdx

@@ -15,6 +15,7 @@
 #include "../host/src/internal.hpp"
 #include "capi_internal.hpp"
 #include "batcher.cuh"
+#include "bruteforce.cuh"
 #include "gpu_runtime.cuh"
 #include "mlp.cuh"
 #include "search.cuh"
@@ -95,6 +96,8 @@ void set_last_error(const std::string& message) { g_error = message; }
 }  // namespace vdx::capi
 
 extern "C" {
+
+void vdx_testing_set_tc_wait_ns(uint64_t ns) { vdx::dev::set_tc_wait_ns(ns); }
 
 const char* vdx_last_error(void) { return g_error.c_str(); }
 const char* vdx_version(void) { return "vdx_b200 0.1.0 (sm_100a)"; }

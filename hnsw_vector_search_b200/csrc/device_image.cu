@@ -278,6 +278,7 @@ void HnswIndex::load_device_image(const std::filesystem::path& path, int device)
     v.links0 = static_cast<const std::uint32_t*>(dg->links0_alloc);
     v.upper_at = static_cast<const std::uint32_t*>(dg->upper_at_alloc);
     v.links_up = static_cast<const std::uint32_t*>(dg->links_up_alloc);
+    gpu::attach_upper_copy(*this, *dg, stream);
     if (!device_mutex_) {
         device_mutex_ = std::make_unique<std::mutex>();
     }

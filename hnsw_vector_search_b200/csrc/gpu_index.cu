@@ -57,7 +57,8 @@ DeviceGraph::~DeviceGraph() {
     int prev = 0;
     cudaGetDevice(&prev);
     cudaSetDevice(device);
-    for (void* p : {vectors_alloc, vectors32_alloc, links0_alloc, upper_at_alloc, links_up_alloc}) {
+    for (void* p : {vectors_alloc, vectors32_alloc, links0_alloc, upper_at_alloc, links_up_alloc,
+                    upper_copy_alloc}) {
         if (p != nullptr) {
             cudaFree(p);
         }
@@ -248,6 +249,124 @@ void raise_status(std::uint32_t code, const char* where) {
     }
 }
 
+namespace {
+
+// Upper blocks with each id's upper_at beside it: block b of `stride` u32 becomes 2 * stride u32.
+__global__ void upper_aug_kernel(const std::uint32_t* links_up, const std::uint32_t* upper_at,
+                                 std::uint32_t* aug, std::uint32_t blocks, std::uint32_t stride,
+                                 std::uint32_t n) {
+    const std::size_t total = static_cast<std::size_t>(blocks) * stride;
+    for (std::size_t x = blockIdx.x * static_cast<std::size_t>(blockDim.x) + threadIdx.x; x < total;
+         x += static_cast<std::size_t>(gridDim.x) * blockDim.x) {
+        const std::size_t b = x / stride;
+        const std::size_t j = x - b * stride;
+        const std::uint32_t id = links_up[x];
+        aug[b * 2 * stride + j] = id;
+        // An id out of range (a corrupted mirror) keeps its slot, which the search reports; its
+        // index is never read.
+        const std::uint32_t ua = id < n ? upper_at[id] : 0u;
+        aug[b * 2 * stride + stride + j] = ua < blocks ? ua : 0u;
+    }
+}
+
+// The traversal row of every node with upper layers, at the index of its first upper block;
+// 16 bytes per thread.
+__global__ void upper_rows_kernel(const unsigned char* vectors, std::uint32_t row_bytes,
+                                  const std::uint32_t* nodes, std::uint32_t count,
+                                  const std::uint32_t* upper_at, unsigned char* rows,
+                                  std::uint32_t blocks) {
+    const std::uint32_t chunks = row_bytes >> 4;
+    const std::size_t total = static_cast<std::size_t>(count) * chunks;
+    for (std::size_t x = blockIdx.x * static_cast<std::size_t>(blockDim.x) + threadIdx.x; x < total;
+         x += static_cast<std::size_t>(gridDim.x) * blockDim.x) {
+        const std::size_t i = x / chunks;
+        const std::size_t c = x - i * chunks;
+        const std::uint32_t node = nodes[i];
+        const std::uint32_t ua = upper_at[node];
+        if (ua < blocks) {
+            const uint4 v = reinterpret_cast<const uint4*>(vectors + static_cast<std::size_t>(node) * row_bytes)[c];
+            reinterpret_cast<uint4*>(rows + static_cast<std::size_t>(ua) * row_bytes)[c] = v;
+        }
+    }
+}
+
+}  // namespace
+
+void attach_upper_copy(const HnswIndex& index, DeviceGraph& dg, cudaStream_t stream) {
+    DeviceGraphView& v = dg.view;
+    if (dg.upper_copy_alloc != nullptr) {
+        cudaFree(dg.upper_copy_alloc);
+        dg.upper_copy_alloc = nullptr;
+    }
+    v.upper_aug = nullptr;
+    v.upper_rows = nullptr;
+    v.l2_window = nullptr;
+    v.l2_window_bytes = 0;
+    const auto levels = index.levels();
+    std::vector<std::uint32_t> nodes;
+    std::uint32_t blocks = 0;
+    std::uint32_t entry_ua = 0;
+    for (std::uint32_t i = 0; i < levels.size(); ++i) {
+        if (i == index.entry_point()) {
+            entry_ua = blocks;
+        }
+        if (levels[i] > 0) {
+            nodes.push_back(i);
+        }
+        blocks += levels[i];
+    }
+    if (blocks == 0 || v.max_level == 0) {
+        return;
+    }
+    const std::size_t aug_bytes = (static_cast<std::size_t>(blocks) * 2 * v.stride_up * 4 + 255) / 256 * 256;
+    const std::size_t rows_bytes = static_cast<std::size_t>(blocks) * v.row_bytes;
+    dg.upper_copy_alloc = device_alloc(aug_bytes + rows_bytes, "upper-layer copy");
+    dg.bytes += aug_bytes + rows_bytes;
+    auto* base = static_cast<unsigned char*>(dg.upper_copy_alloc);
+    void* d_nodes = device_alloc(nodes.size() * 4, "upper-layer nodes");
+    check(cudaMemcpyAsync(d_nodes, nodes.data(), nodes.size() * 4, cudaMemcpyHostToDevice, stream),
+          "upload upper-layer nodes");
+    upper_aug_kernel<<<592, 256, 0, stream>>>(v.links_up, v.upper_at, reinterpret_cast<std::uint32_t*>(base),
+                                             blocks, v.stride_up, v.n);
+    check(cudaGetLastError(), "upper-layer copy");
+    upper_rows_kernel<<<592, 256, 0, stream>>>(static_cast<const unsigned char*>(v.vectors), v.row_bytes,
+                                              static_cast<const std::uint32_t*>(d_nodes),
+                                              static_cast<std::uint32_t>(nodes.size()), v.upper_at,
+                                              base + aug_bytes, blocks);
+    check(cudaGetLastError(), "upper-layer copy");
+    check(cudaStreamSynchronize(stream), "upper-layer copy");
+    cudaFree(d_nodes);
+    v.upper_aug = reinterpret_cast<const std::uint32_t*>(base);
+    v.upper_rows = base + aug_bytes;
+    v.entry_ua = entry_ua;
+    // The L2 set-aside for persisting accesses (a limit of this process's context) is raised,
+    // once per device, to cover the window where the device allows it.
+    int max_persist = 0, max_window = 0;
+    if (cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, dg.device) == cudaSuccess &&
+        cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, dg.device) == cudaSuccess &&
+        max_persist > 0 && max_window > 0) {
+        static std::mutex limit_mutex;
+        static std::size_t limit_set[64] = {};
+        const std::scoped_lock lock(limit_mutex);
+        const std::size_t window = std::min<std::size_t>(static_cast<std::size_t>(max_window),
+                                                         aug_bytes + rows_bytes);
+        const std::size_t want = std::min<std::size_t>(static_cast<std::size_t>(max_persist), window);
+        if (dg.device >= 0 && dg.device < 64) {
+            if (limit_set[dg.device] < want) {
+                if (cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want) == cudaSuccess) {
+                    limit_set[dg.device] = want;
+                } else {
+                    cudaGetLastError();  // no set-aside: the window then only marks the rest streaming
+                }
+            }
+            v.l2_window = base;
+            v.l2_window_bytes = window;
+            v.l2_hit_ratio = std::min(1.0F, static_cast<float>(limit_set[dg.device]) /
+                                                static_cast<float>(window));
+        }
+    }
+}
+
 }  // namespace gpu
 
 namespace {
@@ -431,6 +550,7 @@ std::unique_ptr<DeviceGraph> upload_graph(const HnswIndex& index, int device, Pr
     }
     v.upper_at = static_cast<const std::uint32_t*>(dg->upper_at_alloc);
     v.links_up = static_cast<const std::uint32_t*>(dg->links_up_alloc);
+    gpu::attach_upper_copy(index, *dg, stream);
     return dg;
 }
 

@@ -9,6 +9,11 @@
 #include <stdexcept>
 #include <string>
 
+namespace vdx {
+class HnswIndex;
+struct DeviceGraph;
+}  // namespace vdx
+
 namespace vdx::gpu {
 
 // A failed CUDA call, or no usable device (the C ABI maps it to VDX_ERR_CUDA).
@@ -91,5 +96,11 @@ const void* mapped_host(const void* host);
 Workspace& workspace(int device);
 void reset_small(Workspace& ws);
 void raise_status(std::uint32_t code, const char* where);
+
+// Builds (or rebuilds) the device mirror's upper copy (vdx/device.hpp: the descent's blocks
+// with their upper indices and the rows of nodes with upper layers, one allocation) from the
+// mirror's current links and traversal rows, and sets the mirror's L2 access-policy window over
+// it. Call after the mirror's upper layers or rows change.
+void attach_upper_copy(const HnswIndex& index, DeviceGraph& dg, cudaStream_t stream);
 
 }  // namespace vdx::gpu

@@ -220,6 +220,18 @@ __device__ __forceinline__ float stop_probability(const StopNetView& net, const 
     return 1.0F / (1.0F + __expf(-logit));
 }
 
+// The learned stop's decision at a checkpoint of a stop-only kernel: the features and the
+// network, called out of line so that the walk around it keeps the register allocation of the
+// plain kernels (the network's accumulators and weight loads would otherwise compete with the
+// walk's registers in every expansion). Every lane returns the same answer.
+__device__ __noinline__ bool stop_decision(const StopNetView net, const float* fc, const float* rd,
+                                           int r, int k, const float* hist, int hops, float* h1,
+                                           float threshold, int lane) {
+    float f[kFeatures];
+    stop_features(f, fc, rd, r, k, hist, hops, lane);
+    return stop_probability(net, f, h1, lane) >= threshold;
+}
+
 // Launch bounds. The register-beam kernels over BF16 / FP8 rows need ~10 KB of shared memory
 // per warp, room for 20 resident warps per SM, but at the 128 registers the compiler picks under
 // 256 threads only 16 fit: they are held to 96 registers (blocks of at most 4 warps, 5 per SM;
@@ -409,22 +421,30 @@ __global__ void __launch_bounds__(kMaxThreads<P, kRegR>,
             cur = a.entry_ids[qi];
             curd = a.entry_d[qi];
         } else {
+            // With the upper copy (the descent's blocks with each link's upper index, and the
+            // rows of upper-layer nodes in one L2-resident allocation) the walk reads nothing
+            // else; without it, the graph's own arrays. Same rows, same results.
+            const bool compact = g.upper_aug != nullptr;
+            const unsigned char* const up_rows = compact ? g.upper_rows : vecs;
             if (lane == 0) {
-                fresh[0] = cur;
+                fresh[0] = compact ? g.entry_ua : cur;
             }
             __syncwarp();
-            gather_rows<true>(rows, stride_s, vecs, fresh, 1, g.row_bytes, shift, lane);
+            gather_rows<true>(rows, stride_s, up_rows, fresh, 1, g.row_bytes, shift, lane);
             cp_async_wait<0>();
             __syncwarp();
             curd = lane_distance<P, kL2>(q, rows, g.dim, g.row_bytes);
             ++c_du;
             // cur's first upper block; a move takes the new node's from the candidates' indices,
-            // loaded while their rows are gathered, so a hop waits on one dependent read less.
-            std::uint32_t cur_ua = g.max_level > 0 ? g.upper_at[cur] : 0;
+            // which come with the block (upper copy) or are loaded while their rows are gathered.
+            std::uint32_t cur_ua = g.max_level > 0 ? (compact ? g.entry_ua : g.upper_at[cur]) : 0;
+            // The candidates' upper indices sit after the ids in `fresh` (it holds 2M >= 2 cap_up).
+            std::uint32_t* const fresh_ua = fresh + g.cap_up;
             for (int layer = static_cast<int>(g.max_level); layer >= 1; --layer) {
                 for (std::uint32_t hop = 0; hop <= g.n; ++hop) {
                     const std::uint32_t* block =
-                        g.links_up + static_cast<std::size_t>(cur_ua + layer - 1) * g.stride_up;
+                        compact ? g.upper_aug + static_cast<std::size_t>(cur_ua + layer - 1) * (2 * g.stride_up)
+                                : g.links_up + static_cast<std::size_t>(cur_ua + layer - 1) * g.stride_up;
                     int f = 0;
                     for (std::uint32_t c0 = 0; c0 < g.cap_up; c0 += 32) {
                         const std::uint32_t j = c0 + lane;
@@ -436,7 +456,11 @@ __global__ void __launch_bounds__(kMaxThreads<P, kRegR>,
                         const bool valid = id != kNoId;
                         const std::uint32_t m = __ballot_sync(kFull, valid);
                         if (valid) {
-                            fresh[f + __popc(m & ((1u << lane) - 1u))] = id;
+                            const int at = f + __popc(m & ((1u << lane) - 1u));
+                            fresh[at] = id;
+                            if (compact) {
+                                fresh_ua[at] = block[g.stride_up + j];
+                            }
                         }
                         f += __popc(m);
                     }
@@ -447,10 +471,11 @@ __global__ void __launch_bounds__(kMaxThreads<P, kRegR>,
                     std::uint32_t best_ua = 0;
                     for (int s0 = 0; s0 < f; s0 += rounds_cap) {
                         const int cnt = min(rounds_cap, f - s0);
-                        gather_rows<true>(rows, stride_s, vecs, fresh + s0, cnt, g.row_bytes, shift,
-                                          lane);
+                        gather_rows<true>(rows, stride_s, up_rows, (compact ? fresh_ua : fresh) + s0, cnt,
+                                          g.row_bytes, shift, lane);
                         // Candidates sit on this layer, so each has upper blocks (ids < n: checked).
-                        const std::uint32_t ua = lane < cnt ? g.upper_at[fresh[s0 + lane]] : 0u;
+                        const std::uint32_t ua =
+                            lane < cnt ? (compact ? fresh_ua[s0 + lane] : g.upper_at[fresh[s0 + lane]]) : 0u;
                         cp_async_wait<0>();
                         __syncwarp();
                         const float pd = row_distance<P, kL2>(q, my_row, g.dim, g.row_bytes, half);
@@ -689,7 +714,16 @@ __global__ void __launch_bounds__(kMaxThreads<P, kRegR>,
                 // Every 8 expansions: traces record the state; the stop consults the network
                 // once the k-th distance has been unchanged for stop_gate expansions in a row
                 // (0: at every checkpoint). While it still improves, the beam is not done.
-                if ((hops & 7) == 0 &&
+                if (kLearn == kLearnStop) {
+                    if ((hops & 7) == 0 && hops >= static_cast<int>(a.stop_min_hops) &&
+                        r >= static_cast<int>(k) &&
+                        static_cast<std::uint32_t>(recent_stagnation(hist, hops)) >= a.stop_gate &&
+                        stop_decision(a.stop, fc, rd, r, static_cast<int>(k), hist, hops, h1,
+                                      a.stop_threshold, lane)) {
+                        ++c_stop;
+                        break;
+                    }
+                } else if ((hops & 7) == 0 &&
                     (tracing || static_cast<std::uint32_t>(recent_stagnation(hist, hops)) >= a.stop_gate)) {
                     float f[kFeatures];
                     stop_features(f, fc, rd, r, static_cast<int>(k), hist, hops, lane);
@@ -1006,6 +1040,30 @@ cudaError_t launch_typed(SearchArgs& args, const SearchPlan& plan, std::size_t s
         return cudaSuccess;
     };
     using Kernel = void (*)(SearchArgs);
+    // A launch of a kernel that walks the upper layers carries the graph's L2 access-policy
+    // window over the upper copy (persisting hits, everything else in it streaming).
+    const auto launch_walk = [&](const void* kernel, int blocks) -> cudaError_t {
+        if (args.g.l2_window == nullptr) {
+            reinterpret_cast<Kernel>(const_cast<void*>(kernel))<<<blocks, threads, smem, stream>>>(args);
+            return cudaGetLastError();
+        }
+        cudaLaunchAttribute attr[1] = {};
+        attr[0].id = cudaLaunchAttributeAccessPolicyWindow;
+        attr[0].val.accessPolicyWindow.base_ptr = const_cast<void*>(args.g.l2_window);
+        attr[0].val.accessPolicyWindow.num_bytes = args.g.l2_window_bytes;
+        attr[0].val.accessPolicyWindow.hitRatio = args.g.l2_hit_ratio;
+        attr[0].val.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+        attr[0].val.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(static_cast<unsigned>(blocks));
+        cfg.blockDim = dim3(static_cast<unsigned>(threads));
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = stream;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        void* params[] = {&args};
+        return cudaLaunchKernelExC(&cfg, kernel, params);
+    };
     if (args.entry_ids == nullptr || args.entry_d == nullptr || args.order == nullptr) {
         const void* k0 = pass_kernel<P, kL2, kRegR, 0>(args);
         int blocks = 0;
@@ -1016,9 +1074,8 @@ cudaError_t launch_typed(SearchArgs& args, const SearchPlan& plan, std::size_t s
             return err;
         }
         args.pass = 0;
-        reinterpret_cast<Kernel>(const_cast<void*>(k0))<<<blocks, threads, smem, stream>>>(args);
         g_last_kernels = 1;
-        return cudaGetLastError();
+        return launch_walk(k0, blocks);
     }
     const void* k1 = pass_kernel<P, kL2, kRegR, 1>(args);
     const void* k2 = pass_kernel<P, kL2, kRegR, 2>(args);
@@ -1034,8 +1091,7 @@ cudaError_t launch_typed(SearchArgs& args, const SearchPlan& plan, std::size_t s
         return err;
     }
     args.pass = 1;
-    reinterpret_cast<Kernel>(const_cast<void*>(k1))<<<blocks1, threads, smem, stream>>>(args);
-    if (err = cudaGetLastError(); err != cudaSuccess) {
+    if (err = launch_walk(k1, blocks1); err != cudaSuccess) {
         return err;
     }
     order_kernel<<<1, kOrderThreads, 0, stream>>>(args);

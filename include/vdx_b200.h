@@ -294,6 +294,13 @@ VDX_API vdx_status vdx_bf_search_batch_device(const vdx_bruteforce* index, const
                                               uint32_t method, uint32_t* d_ids, float* d_dists,
                                               uint32_t* d_counts, uint32_t* d_work, void* stream);
 
+/* No reference counterpart. For tests of the device-timeout path only: the limit, in
+ * nanoseconds, of each pipeline wait of the tensor-core brute force's later launches in this
+ * process (0 restores the default of 1 s). A limit shorter than a copy's latency makes the
+ * launch give up (VDX_ERR_DEVICE_TIMEOUT) after draining its own copies and tensor-core work
+ * with the full 1 s bound and freeing its tensor memory. */
+VDX_API void vdx_testing_set_tc_wait_ns(uint64_t ns);
+
 /* --- Host helpers (the distance kernels' order, the file checksum) -------------------------- */
 
 /* kernels::active().l2_squared / inner_product: include/vecdex/kernels.hpp:31 */

@@ -39,6 +39,18 @@ def build(ref: bool = True) -> None:
         subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF_ROOT={root}"], check=True)
 
 
+INTEGRATION_BIN = HERE / "_ref" / "gpu_searcher"
+
+
+def build_integration() -> bool:
+    """Compiles tests/integration/gpu_searcher.cpp (the vecdex-side C++ caller of the C ABI)
+    against the reference's headers when they are present; True when the program exists."""
+    root = ref_root()
+    if root.joinpath("include", "vecdex", "hnsw.hpp").exists() and REF_LIB.exists():
+        subprocess.run(["make", "-s", "-C", str(HERE), "integration", f"REF_ROOT={root}"], check=True)
+    return INTEGRATION_BIN.exists()
+
+
 def _p(a: np.ndarray) -> int:
     return a.ctypes.data
 

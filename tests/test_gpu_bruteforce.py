@@ -108,6 +108,8 @@ def test_tensor_core_equals_exact_at_scale(gpu, metric, make):
     for k in (1, 10):
         a = bf.search_batch(queries, k, method="exact")
         b = bf.search_batch(queries, k, method="tensor_core")
+        if make == "sift":
+            assert gpu.BruteForceIndex.last_uncertified() == 0
         np.testing.assert_array_equal(a[2], b[2])
         np.testing.assert_array_equal(a[0], b[0])
         np.testing.assert_array_equal(a[1].view(np.uint32), b[1].view(np.uint32))
@@ -121,6 +123,9 @@ def test_tensor_core_matches_reference(gpu, orc):
     bf = gpu.BruteForceIndex(128)
     bf.add(base)
     a = bf.search_batch(queries, 10, method="tensor_core")
+    # Integer data: the tensor cores' scores are exact, so every query is certified and none
+    # falls back to the exact kernel.
+    assert gpu.BruteForceIndex.last_uncertified() == 0
     b = ref.search_batch(queries, 10)
     np.testing.assert_array_equal(a[0], b[0])
     np.testing.assert_array_equal(a[1].view(np.uint32), b[1].view(np.uint32))
@@ -146,3 +151,28 @@ def test_concurrent_searches_with_different_k(gpu, method):
             got = job.result()
             np.testing.assert_array_equal(got[0], want[k][0])
             np.testing.assert_array_equal(got[1].view(np.uint32), want[k][1].view(np.uint32))
+
+
+def test_tensor_core_timeout_releases_everything_and_the_next_call_succeeds(gpu):
+    """The timeout path of the tensor-core kernel's bounded waits, made to run out on purpose
+    without any fault: with a pipeline-wait limit of 1 ns every CTA gives up at its first wait
+    for a copy or an MMA, drains its own copies and MMAs (those waits keep the full 1 s bound),
+    frees its tensor memory and returns; the call reports VDX_ERR_DEVICE_TIMEOUT. With the
+    default limit back, the next calls succeed with the exact results (tensor memory that was
+    not freed would make later allocations fail or block)."""
+    from hnsw_vector_search_b200 import datasets as ds
+    base, queries = ds.config_sift_like(rows=20_000, n_queries=300)
+    bf = gpu.BruteForceIndex(128)
+    bf.add(base)
+    want = bf.search_batch(queries, 10, method="exact")
+    lib = gpu.lib()
+    try:
+        lib.vdx_testing_set_tc_wait_ns(1)
+        with pytest.raises(gpu.DeviceTimeout, match="timed out"):
+            bf.search_batch(queries, 10, method="tensor_core")
+    finally:
+        lib.vdx_testing_set_tc_wait_ns(0)
+    for _ in range(3):
+        got = bf.search_batch(queries, 10, method="tensor_core")
+        np.testing.assert_array_equal(got[0], want[0])
+        np.testing.assert_array_equal(got[1].view(np.uint32), want[1].view(np.uint32))
