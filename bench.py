@@ -283,7 +283,8 @@ def main():
     ap.add_argument("--mode", default="fp32",
                     choices=["fp32", "bf16", "fp8", "bf_tc", "bf_exact", "mlp", "build"])
     ap.add_argument("--ef", type=int, default=32)
-    ap.add_argument("--study", choices=["uneven", "precision", "build", "device_image", "learned"],
+    ap.add_argument("--study", choices=["uneven", "precision", "build", "device_image", "learned",
+                                        "ip_graph"],
                     help="instead of the headline: the uneven-batch stream or the precision study")
     ap.add_argument("--rows", type=int, default=0, help="base rows of a study (0: its default)")
     args = ap.parse_args()
@@ -325,6 +326,9 @@ def main():
         return
     if args.study == "learned":
         study_learned(args, v, torch)
+        return
+    if args.study == "ip_graph":
+        study_ip_graph(args, v, torch)
         return
     base, queries = workload()
     cpu = None
@@ -1043,6 +1047,50 @@ def study_learned(args, v, torch):
                       "train_seconds_with_traces": round(train_s, 2),
                       "loss_per_epoch": [round(float(l), 5) for l in losses],
                       "plain": plain, "learned": points}), flush=True)
+
+
+def study_ip_graph(args, v, torch):
+    """How good an HNSW graph gets on the uneven-batch data (96-d inner product, 4,096 clusters
+    with log-normal scales, M 24, ef_construction 200): this library's GPU build against the
+    reference's own parallel build on all host cores, same rows (default 1M), each graph's
+    nodes reachable from the entry point, mean layer-0 degree, and the recall@10 of the GPU
+    search of 2,000 queries of the same mixture at several ef, judged by exact brute force."""
+    from hnsw_vector_search_b200.datasets import scaled_clusters
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as o
+    n = args.rows or 1_000_000
+    base = scaled_clusters(n, 96, 4096, seed=51, centers_seed=151)
+    queries = scaled_clusters(2000, 96, 4096, seed=52, centers_seed=151)
+    exact = v.BruteForceIndex(96, "ip")
+    exact.add(base)
+    truth, _, _ = exact.search_batch(queries, K)
+    del exact
+    efs = (10, 32, 64, 128, 256, 512, 656)
+    out = {}
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    g = v.HnswIndex(96, "ip", M=24, ef_construction=EF_CONSTRUCTION, seed=SEED)
+    g.add(base, device=0)
+    torch.cuda.synchronize()
+    graphs = [("gpu_build", g, time.perf_counter() - t0)]
+    t0 = time.perf_counter()
+    ref = o.RefHnsw(96, 1, 24, EF_CONSTRUCTION, SEED)
+    ref.add(base, threads=0)
+    ref_s = time.perf_counter() - t0
+    path = CACHE / f"ip_graph_{n}_reference.vdx"
+    CACHE.mkdir(exist_ok=True)
+    ref.save(path)
+    del ref
+    graphs.append(("reference_parallel_build", v.HnswIndex.load(path), ref_s))
+    for name, ix, secs in graphs:
+        rep = ix.inspect()
+        out[name] = {"build_seconds": round(secs, 1), "reachable": rep["reachable"],
+                     "mean_degree0": round(rep["mean_degree0"], 3), "violations": rep["violations"],
+                     "recall_at_10": {ef: round(recall_at_10(ix.search_batch(queries, K, ef)[0], truth), 4)
+                                      for ef in efs}}
+    path.unlink()
+    print(json.dumps({"study": "ip_graph", "workload": f"{n} x 96 IP, 4,096 clusters (log-normal "
+                      f"scales), M24 efc{EF_CONSTRUCTION}, 2,000 queries", "graphs": out}), flush=True)
 
 
 def study_precision(args, v, torch):
