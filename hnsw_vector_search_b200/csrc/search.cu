@@ -111,21 +111,24 @@ __device__ __forceinline__ bool first_visit_global(unsigned long long* table, st
 
 constexpr int kFeatures = 12;
 constexpr int kHidden = 64;
-constexpr int kHist = 32;  // ring of the k-th distance after each expansion
+constexpr int kHist = 8;   // ring of the k-th distance after every 4th expansion
 
 __device__ __forceinline__ float sgnlog(float x) { return copysignf(log1pf(fabsf(x)), x); }
 
 // The 12 features of a query's search state after `hops` expansions (the model's inputs):
 //   0 log(1 + |q|)                      1 signed log of the layer-0 entry distance
 //   2 log(1 + (d_k - d_1) / |d_1|)      3..5 relative drop of d_k over the last 4 / 8 / 16
-//   6 log(1 + hops)                     7 log(1 + expansions since d_k last improved)
+//   6 log(1 + hops)                     7 log(1 + expansions since d_k last changed, <= 31)
 //   8..11 query projections
 // None depends on ef, so a model trained on traces at one ef cap reads the same features at
 // another. Called by every lane (the ballot of feature 7 needs the whole warp).
 // `fc` holds the query's constant features: [0] |q|, [1] layer-0 entry distance, [2..5] the
 // projections.
+// `ring` holds d_k after every 4th expansion (ring[(h / 4) % 8] after expansion h, h > 0), and
+// `unchanged` counts the expansions since d_k last changed (a candidate kept at a position below
+// k), so the walk writes shared memory only every 4th expansion.
 __device__ __forceinline__ void stop_features(float* f, const float* fc, const float* rd, int r,
-                                              int k, const float* hist, int hops, int lane) {
+                                              int k, const float* ring, int hops, int unchanged) {
     const float qlen = fc[0];
     const float d_entry = fc[1];
     const int kk = r < k ? r : k;
@@ -137,34 +140,19 @@ __device__ __forceinline__ void stop_features(float* f, const float* fc, const f
     const int ws[3] = {4, 8, 16};
 #pragma unroll
     for (int w = 0; w < 3; ++w) {
-        const int back = hops - 1 - ws[w];
-        const float prev = hist[(back > 0 ? back : 0) & (kHist - 1)];
+        const int back = hops - ws[w] > 4 ? hops - ws[w] : 4;  // the earliest sample is after 4
+        const float prev = ring[(back >> 2) & 7];
         const float drop = (prev - dk) / (fabsf(dk) + 1e-6F * (1.0F + fabsf(dk)));
         f[3 + w] = fminf(fmaxf(drop, -10.0F), 10.0F);
     }
     f[6] = log1pf(static_cast<float>(hops));
-    // hist[(hops - 1 - j) % 32] is d_k after expansion hops - j; count the latest expansions
-    // that left it unchanged (at most 31).
-    const int span = hops < kHist ? hops : kHist;
-    const bool same = lane < span && hist[(hops - 1 - lane) & (kHist - 1)] == dk;
-    const std::uint32_t run = __ballot_sync(kFull, same);
-    const int unchanged = (~run == 0u ? 32 : __ffs(~run) - 1) - 1;
-    f[7] = log1pf(static_cast<float>(unchanged > 0 ? unchanged : 0));
+    f[7] = log1pf(static_cast<float>(unchanged < 31 ? unchanged : 31));
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
         f[8 + i] = fc[2 + i];
     }
 }
 
-// Expansions in a row, ending with the latest one, that left the k-th distance unchanged
-// (0 to 3): the stop's gate reads no more than that.
-__device__ __forceinline__ int recent_stagnation(const float* hist, int hops) {
-    const float a = hist[(hops - 1) & (kHist - 1)];
-    const float b = hist[(hops - 2) & (kHist - 1)];
-    const float c = hist[(hops - 3) & (kHist - 1)];
-    const float d = hist[(hops - 4) & (kHist - 1)];
-    return a != b ? 0 : (b != c ? 1 : (c != d ? 2 : 3));
-}
 
 // P(converged) of the network for features f (identical in every lane); h1 is 64 floats of
 // per-warp shared scratch. Lane L computes hidden units L and L + 32 of both layers from the
@@ -225,10 +213,10 @@ __device__ __forceinline__ float stop_probability(const StopNetView& net, const 
 // plain kernels (the network's accumulators and weight loads would otherwise compete with the
 // walk's registers in every expansion). Every lane returns the same answer.
 __device__ __noinline__ bool stop_decision(const StopNetView net, const float* fc, const float* rd,
-                                           int r, int k, const float* hist, int hops, float* h1,
-                                           float threshold, int lane) {
+                                           int r, int k, const float* ring, int hops, int unchanged,
+                                           float* h1, float threshold, int lane) {
     float f[kFeatures];
-    stop_features(f, fc, rd, r, k, hist, hops, lane);
+    stop_features(f, fc, rd, r, k, ring, hops, unchanged);
     return stop_probability(net, f, h1, lane) >= threshold;
 }
 
@@ -280,7 +268,7 @@ __global__ void __launch_bounds__(kMaxThreads<P, kRegR>,
     unsigned char* rows = ws + a.off_rows;
     std::uint32_t* fresh = reinterpret_cast<std::uint32_t*>(ws + a.off_fresh);
     int* ap = reinterpret_cast<int*>(ws + a.off_ap);
-    float* hist = reinterpret_cast<float*>(ws + a.off_hist);  // kHist k-th distances
+    float* hist = reinterpret_cast<float*>(ws + a.off_hist);  // kHist sampled k-th distances
     float* h1 = hist + kHist;                                 // kHidden network scratch
     float* fc = h1 + kHidden;                                 // the query's constant features
 
@@ -563,6 +551,7 @@ __global__ void __launch_bounds__(kMaxThreads<P, kRegR>,
             fc[1] = curd;  // the layer-0 entry distance
         }
         int hops = 0;
+        int last_change = 0;  // learned stop / traces: the expansion that last changed d_k
         for (std::uint32_t step = 0; step <= g.n; ++step) {
             int p;
             std::uint32_t node;
@@ -637,6 +626,7 @@ __global__ void __launch_bounds__(kMaxThreads<P, kRegR>,
             }
             __syncwarp();
             c_lw += 1 + count;
+            int kept_low = 0x7FFFFFFF;  // the lowest position a candidate was kept at
             for (int s0 = 0; s0 < f; s0 += rounds_cap) {
                 const int cnt = min(rounds_cap, f - s0);
                 gather_rows(rows, stride_s, vecs, fresh + s0, cnt, g.row_bytes, shift, lane);
@@ -691,6 +681,9 @@ __global__ void __launch_bounds__(kMaxThreads<P, kRegR>,
                     low = merge_round(rd, rid, r, ef, my_d, my_id, valid, ap, lane, c_dup);
                 }
                 scan = min(scan, low);
+                if constexpr (kLearn != kLearnNone) {
+                    kept_low = min(kept_low, low);
+                }
             }
             if (f == 0) {
                 // Nothing scored: the next expansion is R's first unexpanded entry.
@@ -707,26 +700,33 @@ __global__ void __launch_bounds__(kMaxThreads<P, kRegR>,
             ++hops;
             if (learned || tracing) {
                 const int kk = r < static_cast<int>(k) ? r : static_cast<int>(k);
-                if (lane == 0) {
-                    hist[(hops - 1) & (kHist - 1)] = rd[kk - 1];
+                // d_k changed when a candidate was kept above it (the merge's lowest kept
+                // position); its value is sampled into the ring after every 4th expansion.
+                if (kept_low < kk) {
+                    last_change = hops;
                 }
-                __syncwarp();
+                if ((hops & 3) == 0) {
+                    if (lane == 0) {
+                        hist[(hops >> 2) & 7] = rd[kk - 1];
+                    }
+                    __syncwarp();
+                }
+                const int unchanged = hops - last_change;
                 // Every 8 expansions: traces record the state; the stop consults the network
                 // once the k-th distance has been unchanged for stop_gate expansions in a row
                 // (0: at every checkpoint). While it still improves, the beam is not done.
                 if (kLearn == kLearnStop) {
                     if ((hops & 7) == 0 && hops >= static_cast<int>(a.stop_min_hops) &&
-                        r >= static_cast<int>(k) &&
-                        static_cast<std::uint32_t>(recent_stagnation(hist, hops)) >= a.stop_gate &&
-                        stop_decision(a.stop, fc, rd, r, static_cast<int>(k), hist, hops, h1,
+                        r >= static_cast<int>(k) && static_cast<std::uint32_t>(unchanged) >= a.stop_gate &&
+                        stop_decision(a.stop, fc, rd, r, static_cast<int>(k), hist, hops, unchanged, h1,
                                       a.stop_threshold, lane)) {
                         ++c_stop;
                         break;
                     }
                 } else if ((hops & 7) == 0 &&
-                    (tracing || static_cast<std::uint32_t>(recent_stagnation(hist, hops)) >= a.stop_gate)) {
+                    (tracing || static_cast<std::uint32_t>(unchanged) >= a.stop_gate)) {
                     float f[kFeatures];
-                    stop_features(f, fc, rd, r, static_cast<int>(k), hist, hops, lane);
+                    stop_features(f, fc, rd, r, static_cast<int>(k), hist, hops, unchanged);
                     if (tracing && trace_points < a.trace.max_points) {
                         const std::size_t at = static_cast<std::size_t>(qi) * a.trace.max_points + trace_points;
                         if (lane < kFeatures) {

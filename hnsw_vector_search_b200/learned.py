@@ -30,7 +30,7 @@ from .recall import recall_at_k
 
 FEATURES = 12
 PARAMS = 5057
-MODEL_VERSION = 3
+MODEL_VERSION = 4
 
 
 def _bind():
