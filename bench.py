@@ -330,20 +330,31 @@ def main():
     if args.study == "ip_graph":
         study_ip_graph(args, v, torch)
         return
-    base, queries = workload()
+    # Rank 0 makes (or finds) every cached input first — the data, the reference's graph, the
+    # ground truth, the learned model — and the other ranks read them after a barrier, so no two
+    # ranks write the same cache file.
     cpu = None
     if rank == 0:
+        base, queries = workload()
         graph = reference_graph(base)
+        truth = ground_truth(base, queries)
     if pg is not None:
         pg.barrier()
-    graph = reference_graph(base)
-    truth = ground_truth(base, queries)
+    if rank != 0:
+        base, queries = workload()
+        graph = reference_graph(base)
+        truth = ground_truth(base, queries)
 
     ix = v.HnswIndex.load(graph)
     modes = [("fp32", {}), ("bf16", {"precision": "bf16", "rerank": 40})]
     for _, o in modes:
         ix.upload(local, o.get("precision", "fp32"))
-    learned_info = learned_mode(v, torch, ix, base, graph, local)
+    if rank == 0:
+        learned_info = learned_mode(v, torch, ix, base, graph, local)
+    if pg is not None:
+        pg.barrier()
+    if rank != 0:
+        learned_info = learned_mode(v, torch, ix, base, graph, local)
     modes.append(("learned_bf16", {"precision": "bf16", "rerank": 40, "learned_stop": True,
                                    "stop_threshold": learned_info["threshold"],
                                    "stop_gate": learned_info["gate"]}))
