@@ -8,11 +8,11 @@
 //    stored vectors through shared memory in tiles of 128 rows (N), K in 64-element swizzled
 //    chunks. One thread issues TMA loads (no multicast), one thread issues
 //    tcgen05.mma.kind::f16 (BF16 x BF16 -> FP32 in TMEM, the terms hi*hi + hi*lo + lo*hi when
-//    the data needs them), and four warps read the 128 x 128 FP32 tile out of TMEM (double
-//    buffered, so the next tile's MMAs overlap), turn scores into distances
-//    (||q||^2 + ||x||^2 - 2 q.x, or 1 - q.x) and keep each query's best `kc` candidates of the
-//    chunk in shared memory (one query per thread).
-// 3. merge (bf_tc_merge_kernel): per query, the best `kc` candidates over all chunks are
+//    the data needs them), and eight warps read the 128 x 128 FP32 tile out of TMEM (double
+//    buffered, so the next tile's MMAs overlap), score it (2 q.x - ||x||^2, or q.x) and keep
+//    each query's best `kc` candidates of the chunk in shared memory (one query per thread and
+//    column half), starting from the best bound the query's other lists have published.
+// 3. merge (bf_tc_merge_kernel): per query, the best `kc` candidates over all lists are
 //    re-scored with the reference's exact FP32 order (lane_distance) and sorted by `closer`.
 //    The query is certified when its k-th exact distance is below every excluded vector's
 //    lowest possible exact distance (the smallest excluded approximate distance minus the
@@ -170,6 +170,14 @@ __device__ __forceinline__ float max3(float a, float b, float c) {
     asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
     return d;
 }
+// 32 consecutive score offsets (one 32-column group), as eight broadcast 16-byte loads.
+__device__ __forceinline__ void load_bias(float4 (&v)[8], const float* src) {
+    const float4* s = reinterpret_cast<const float4*>(src);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        v[i] = __ldg(s + i);
+    }
+}
 
 // Order-preserving map of floats to u32 (so atomicMax on the key is max on the float).
 __device__ __forceinline__ std::uint32_t float_to_key(float f) {
@@ -185,11 +193,57 @@ __device__ __forceinline__ float key_to_float(std::uint32_t k) {
     return __uint_as_float((k & 0x80000000u) ? (k & 0x7FFFFFFFu) : ~k);
 }
 
+// One score against a thread's candidate list (column e of [kc][128] arrays, best first, ties
+// by the lower id). `thr` / `thr_i` is the acceptance bound (kNoId: ties with it are accepted);
+// it only rises, to the list's kc-th once the list is full.
+__device__ __forceinline__ void consider(float v, std::uint32_t id, float* list_d,
+                                         std::uint32_t* list_i, std::uint32_t e, std::uint32_t kc,
+                                         std::uint32_t& count, float& thr, std::uint32_t& thr_i) {
+    if (!(v > thr || (v == thr && id < thr_i))) {
+        return;
+    }
+    std::uint32_t pos = count < kc ? count : kc - 1;
+    while (pos > 0) {
+        const float pv = list_d[(pos - 1) * kBM + e];
+        const std::uint32_t pi = list_i[(pos - 1) * kBM + e];
+        if (!(v > pv || (v == pv && id < pi))) {
+            break;
+        }
+        list_d[pos * kBM + e] = pv;
+        list_i[pos * kBM + e] = pi;
+        --pos;
+    }
+    list_d[pos * kBM + e] = v;
+    list_i[pos * kBM + e] = id;
+    if (count < kc) {
+        ++count;
+    }
+    if (count == kc) {
+        const float kth = list_d[(kc - 1) * kBM + e];
+        const std::uint32_t kth_i = list_i[(kc - 1) * kBM + e];
+        if (kth > thr || (kth == thr && thr_i == kNoId)) {
+            thr = kth;
+            thr_i = kth_i;
+        }
+    }
+}
+
 // -------------------------------------------------------------------------------------------
 // Kernel parameters
 
+// Work split: the stored rows' tpq tiles of 128 are cut into `nchunks` runs of equal length (to
+// a tile); a work item is one (query tile, chunk) pair, item = chunk * qtiles + query tile, and
+// CTA b takes items b, b + grid, b + 2 grid, ... So the CTAs of one wave stream the same one to
+// three chunks side by side (a row tile is read from HBM about once per wave and then served by
+// L2), and a query's chunks are taken in order, each list starting from the best bound that the
+// query's other lists have published (`floor_key`).
+__host__ __device__ inline std::uint32_t chunk_begin(std::uint32_t ch, std::uint32_t tpq,
+                                                     std::uint32_t nchunks) {
+    return static_cast<std::uint32_t>(static_cast<std::uint64_t>(ch) * tpq / nchunks);
+}
+
 struct TcParams {
-    std::uint32_t nq, n, dim, kchunks, qtiles, nchunks, chunk_rows, kc, stages, metric;
+    std::uint32_t nq, n, dim, kchunks, qtiles, nchunks, tpq, kc, stages, metric;
     std::uint32_t halves;                 // epilogue warps per TMEM lane quarter (column halves)
     std::uint32_t base_lo;                // the stored vectors have nonzero lo parts
     const std::uint32_t* query_flags;     // bit 0: some query has a nonzero lo part
@@ -198,7 +252,7 @@ struct TcParams {
     std::uint32_t* cand_ids;              // [nq][nchunks * halves][kc]
     float* cand_d;
     float* cand_tau;                      // [nq][nchunks * halves]
-    std::uint32_t* floor_key;             // [nq] best kc-th score of any finished chunk (ordered key)
+    std::uint32_t* floor_key;             // [nq] best kc-th score any list holds (ordered key)
     std::uint32_t* error;                 // status word: 5 on a timeout
     std::uint64_t wait_ns;                // limit of each pipeline wait (the drains keep kWaitNs)
     std::uint32_t off_b, off_lists, off_bar;  // smem offsets from the 1024-aligned base
@@ -288,9 +342,9 @@ __global__ void __launch_bounds__(kThreads, 1)
                 }
             }
             ++a_loads;
-            const std::uint32_t row0 = ch * p.chunk_rows;
-            const std::uint32_t rows = min(p.chunk_rows, p.n - row0);
-            const std::uint32_t tiles = (rows + kBN - 1) / kBN;
+            const std::uint32_t t0 = chunk_begin(ch, p.tpq, p.nchunks);
+            const std::uint32_t row0 = t0 * kBN;
+            const std::uint32_t tiles = chunk_begin(ch + 1, p.tpq, p.nchunks) - t0;
             for (std::uint32_t t = 0; t < tiles; ++t, ++it) {
                 const std::uint32_t s = it % S;
                 const std::uint32_t ph = (it / S) & 1u;
@@ -329,9 +383,9 @@ __global__ void __launch_bounds__(kThreads, 1)
         bool ok = true;
         for (std::uint32_t item = blockIdx.x; ok && item < items; item += gridDim.x, ++item_idx) {
             const std::uint32_t ch = item / p.qtiles;
-            const std::uint32_t row0 = ch * p.chunk_rows;
-            const std::uint32_t rows = min(p.chunk_rows, p.n - row0);
-            const std::uint32_t tiles = (rows + kBN - 1) / kBN;
+            const std::uint32_t t0 = chunk_begin(ch, p.tpq, p.nchunks);
+            const std::uint32_t row0 = t0 * kBN;
+            const std::uint32_t tiles = chunk_begin(ch + 1, p.tpq, p.nchunks) - t0;
             if (!mbar_wait(a_full, item_idx & 1u, abort_flag, p.wait_ns)) {
                 fail();
                 ok = false;
@@ -377,15 +431,16 @@ __global__ void __launch_bounds__(kThreads, 1)
     } else if (warp >= 4 && static_cast<std::uint32_t>(warp - 4) < 4 * p.halves) {
         // Epilogue: thread e owns query row e of the tile (TMEM lane e) in column half `half`
         // of every tile (with halves = 2, two warps per TMEM lane quarter split the 128 columns,
-        // so two warps per scheduler hide each other's latency), with its own candidate list
-        // (the merge treats each half's list like a chunk of its own). It works in score space,
-        // t = 2 q.x - ||x||^2 (L2) or t = q.x (inner product), larger is closer; the per-row
-        // offset (-||x||^2, or -0; -inf for padding rows) is read 32 at a time with broadcast
-        // 16-byte loads, and a group of 32 scores enters the insertion path only if its best
-        // score can beat the list's current worst.
+        // so two warps per scheduler hide each other's latency), with its own candidate list per
+        // item (the merge treats each half's list like a chunk of its own). It works in score
+        // space, t = 2 q.x - ||x||^2 (L2) or t = q.x (inner product), larger is closer; the
+        // per-row offset (-||x||^2, or -0; -inf for padding rows) is read 32 at a time with
+        // broadcast 16-byte loads issued one group ahead, and a group of 32 scores enters the
+        // insertion path only if its best score can beat the list's current bound.
         const std::uint32_t e = static_cast<std::uint32_t>((warp & 3) * 32 + lane);
         const std::uint32_t half = static_cast<std::uint32_t>(warp - 4) >> 2;
         const std::uint32_t groups = (kBN / 32) / p.halves;  // 32-column groups per half
+        const std::uint32_t g0 = half * groups;
         const std::uint32_t lists = p.nchunks * p.halves;
         float* list_d = reinterpret_cast<float*>(base + p.off_lists + half * p.kc * kBM * 8);  // [kc][128]
         std::uint32_t* list_i = reinterpret_cast<std::uint32_t*>(base + p.off_lists + half * p.kc * kBM * 8 +
@@ -394,21 +449,23 @@ __global__ void __launch_bounds__(kThreads, 1)
         const bool l2 = p.metric == 0;
         const float c2 = l2 ? 2.0F : 1.0F;
         std::uint32_t acc_it = 0;
-        for (std::uint32_t item = blockIdx.x; item < items; item += gridDim.x) {
+        bool ok = true;
+        for (std::uint32_t item = blockIdx.x; ok && item < items; item += gridDim.x) {
             const std::uint32_t qt = item % p.qtiles;
             const std::uint32_t ch = item / p.qtiles;
             const std::uint32_t row = qt * kBM + e;
             const bool live = row < p.nq;
-            const std::uint32_t row0 = ch * p.chunk_rows;
-            const std::uint32_t rows = min(p.chunk_rows, p.n - row0);
-            const std::uint32_t tiles = (rows + kBN - 1) / kBN;
+            const std::uint32_t t0 = chunk_begin(ch, p.tpq, p.nchunks);
+            const std::uint32_t row0 = t0 * kBN;
+            const std::uint32_t tiles = chunk_begin(ch + 1, p.tpq, p.nchunks) - t0;
             std::uint32_t count = 0;
-            // Scores at or below `floor` cannot reach the global best kc: another chunk already
-            // holds kc better ones (its list is part of the merge).
-            const float floor = live ? key_to_float(p.floor_key[row]) : INFINITY;
-            float thr = floor;          // acceptance bound: the floor, then the list's kc-th
+            // Scores at or below `floor` cannot reach the global best kc: another list already
+            // holds kc better ones (every list is part of the merge).
+            float floor = live ? key_to_float(__ldcg(p.floor_key + row)) : INFINITY;
+            float thr = floor;            // acceptance bound: the floor, then the list's kc-th
             std::uint32_t thr_i = kNoId;  // kNoId: ties with the bound are accepted
-            bool ok = true;
+            float4 nb[8];
+            load_bias(nb, p.xnorm + row0 + g0 * 32);
             for (std::uint32_t t = 0; t < tiles; ++t, ++acc_it) {
                 const std::uint32_t b = acc_it & 1u;
                 if (!mbar_wait(tfull0 + 8 * b, (acc_it >> 1) & 1u, abort_flag, p.wait_ns)) {
@@ -417,71 +474,98 @@ __global__ void __launch_bounds__(kThreads, 1)
                     break;
                 }
                 tc_fence_after();
-                for (std::uint32_t cc = half * groups; cc < (half + 1) * groups; ++cc) {
+                for (std::uint32_t g = 0; g < groups; ++g) {
+                    const std::uint32_t cc = g0 + g;
+                    const std::uint32_t id0 = row0 + t * kBN + cc * 32;
+                    // The offsets of the next group (this tile's next, or the next tile's first;
+                    // the current group again after the item's last), in flight while this
+                    // group's scores are read and scored.
+                    const std::uint32_t nxt = g + 1 < groups ? id0 + 32
+                                              : t + 1 < tiles ? row0 + (t + 1) * kBN + g0 * 32
+                                                              : id0;
+                    float4 nx[8];
+                    load_bias(nx, p.xnorm + nxt);
                     std::uint32_t r[32];
                     tmem_ld32(tmem + lane_base + b * kBN + cc * 32, r);
-                    if (cc == (half + 1) * groups - 1) {
+                    if (g == groups - 1) {
                         tc_fence_before();
                         mbar_arrive(tempty0 + 8 * b);
                     }
-                    const std::uint32_t id0 = row0 + t * kBN + cc * 32;
-                    const float4* nb4 = reinterpret_cast<const float4*>(p.xnorm + id0);
                     // t = c * s + nb with c = 2 (L2) or 1 and nb = -||x||^2 (L2), -0 (inner
                     // product) or -inf (padding rows): two scores per f32x2 FMA, each rounded
                     // like a scalar fmaf. Everything stays in registers (static indices only).
                     float sc[32];
 #pragma unroll
                     for (int q4 = 0; q4 < 8; ++q4) {
-                        const float4 bv = __ldg(nb4 + q4);
                         fma2(sc[4 * q4], sc[4 * q4 + 1], c2, __uint_as_float(r[4 * q4]),
-                             __uint_as_float(r[4 * q4 + 1]), bv.x, bv.y);
+                             __uint_as_float(r[4 * q4 + 1]), nb[q4].x, nb[q4].y);
                         fma2(sc[4 * q4 + 2], sc[4 * q4 + 3], c2, __uint_as_float(r[4 * q4 + 2]),
-                             __uint_as_float(r[4 * q4 + 3]), bv.z, bv.w);
+                             __uint_as_float(r[4 * q4 + 3]), nb[q4].z, nb[q4].w);
                     }
-                    // Best of the 32 with three-input max; most groups stop here.
-                    float m8[11];
+#pragma unroll
+                    for (int q4 = 0; q4 < 8; ++q4) {
+                        nb[q4] = nx[q4];
+                    }
+                    // Best of each triple, then of the 32, with three-input max; most groups
+                    // stop here.
+                    float m3[11];
 #pragma unroll
                     for (int i = 0; i < 10; ++i) {
-                        m8[i] = max3(sc[3 * i], sc[3 * i + 1], sc[3 * i + 2]);
+                        m3[i] = max3(sc[3 * i], sc[3 * i + 1], sc[3 * i + 2]);
                     }
-                    m8[10] = fmaxf(sc[30], sc[31]);
-                    const float mx = max3(max3(m8[0], m8[1], m8[2]), max3(m8[3], m8[4], m8[5]),
-                                          max3(max3(m8[6], m8[7], m8[8]), m8[9], m8[10]));
+                    m3[10] = fmaxf(sc[30], sc[31]);
+                    const float mx = max3(max3(m3[0], m3[1], m3[2]), max3(m3[3], m3[4], m3[5]),
+                                          max3(max3(m3[6], m3[7], m3[8]), m3[9], m3[10]));
                     if (!live || !(mx >= thr)) {
                         continue;
                     }
-                    // Rare path: each score that may qualify, in column order; the bound only
-                    // rises. Static indices keep the scores in registers.
+                    // Rare path, kept small (it runs cold, so its size costs instruction-cache
+                    // misses): the triples whose best may qualify, in column order, each picked
+                    // out of the registers by predicated moves, their scores offered to one copy
+                    // of the insertion code. The bound only rises, so a triple that failed under
+                    // an older bound stays out under a newer one.
+                    std::uint32_t tm = 0;
 #pragma unroll
-                    for (int j = 0; j < 32; ++j) {
-                        const float v = sc[j];
-                        const std::uint32_t id = id0 + static_cast<std::uint32_t>(j);
-                        if (!(v > thr || (v == thr && id < thr_i))) {
-                            continue;
-                        }
-                        std::uint32_t pos = count < p.kc ? count : p.kc - 1;
-                        while (pos > 0) {
-                            const float pv = list_d[(pos - 1) * kBM + e];
-                            const std::uint32_t pi = list_i[(pos - 1) * kBM + e];
-                            if (!(v > pv || (v == pv && id < pi))) {
-                                break;
+                    for (int i = 0; i < 11; ++i) {
+                        tm |= m3[i] >= thr ? 1u << i : 0u;
+                    }
+                    while (tm != 0) {
+                        const int i = __ffs(static_cast<int>(tm)) - 1;
+                        tm &= tm - 1;
+                        float v0 = 0.0F, v1 = 0.0F, v2 = 0.0F;
+#pragma unroll
+                        for (int k = 0; k < 11; ++k) {
+                            if (k == i) {
+                                v0 = sc[3 * k];
+                                v1 = sc[3 * k + 1];
+                                v2 = k < 10 ? sc[3 * k + 2] : 0.0F;
                             }
-                            list_d[pos * kBM + e] = pv;
-                            list_i[pos * kBM + e] = pi;
-                            --pos;
                         }
-                        list_d[pos * kBM + e] = v;
-                        list_i[pos * kBM + e] = id;
-                        if (count < p.kc) {
-                            ++count;
+                        const std::uint32_t idb = id0 + 3u * static_cast<std::uint32_t>(i);
+                        const int width = i < 10 ? 3 : 2;
+#pragma unroll 1
+                        for (int jj = 0; jj < width; ++jj) {
+                            consider(jj == 0 ? v0 : (jj == 1 ? v1 : v2), idb + static_cast<std::uint32_t>(jj),
+                                     list_d, list_i, e, p.kc, count, thr, thr_i);
                         }
-                        if (count == p.kc) {
-                            const float kth = list_d[(p.kc - 1) * kBM + e];
-                            const std::uint32_t kth_i = list_i[(p.kc - 1) * kBM + e];
-                            if (kth > thr || (kth == thr && thr_i == kNoId)) {
-                                thr = kth;
-                                thr_i = kth_i;
-                            }
+                    }
+                }
+                if (live && (t & 31u) == 31u) {
+                    // Every 32 tiles: publish this list's kc-th (its kc entries only improve)
+                    // and take up a better floor from the query's other lists.
+                    std::uint32_t key;
+                    if (count == p.kc) {
+                        const std::uint32_t mine = float_to_key(list_d[(p.kc - 1) * kBM + e]);
+                        key = max(atomicMax(p.floor_key + row, mine), mine);
+                    } else {
+                        key = __ldcg(p.floor_key + row);
+                    }
+                    const float fl = key_to_float(key);
+                    if (fl > floor) {
+                        floor = fl;
+                        if (fl > thr) {
+                            thr = fl;
+                            thr_i = kNoId;
                         }
                     }
                 }
@@ -499,8 +583,9 @@ __global__ void __launch_bounds__(kThreads, 1)
                     p.cand_d[at + i] = i < count ? (l2 ? __fsub_rn(qn, v) : __fsub_rn(1.0F, v)) : INFINITY;
                     p.cand_ids[at + i] = i < count ? list_i[i * kBM + e] : kNoId;
                 }
-                // Every excluded row of this chunk scored at most `thr` (the floor, or the full
-                // list's kc-th): no excluded distance is below the matching distance.
+                // Every excluded row of this item scored at most `thr` (the floor, or the full
+                // list's kc-th, whichever is higher; both only rose): no excluded distance is
+                // below the matching distance.
                 const float bound = count == p.kc ? fmaxf(thr, floor) : floor;
                 p.cand_tau[list] =
                     bound == -INFINITY ? INFINITY : (l2 ? __fsub_rn(qn, bound) : __fsub_rn(1.0F, bound));
@@ -632,7 +717,7 @@ __global__ void bias_kernel(const float* norm, float* bias, std::uint32_t n, std
 // Merge, exact re-rank, certification. One warp per query.
 
 struct MergeParams {
-    std::uint32_t nq, n, dim, row32, nchunks, kc, k, out_stride, metric, dk, terms;
+    std::uint32_t nq, n, dim, row32, lists, kc, k, out_stride, metric, dk, terms;
     const float* queries;          // normalized FP32 rows [nq][row32]
     const std::uint8_t* valid;
     const std::uint8_t* q_exact;
@@ -686,16 +771,16 @@ __global__ void bf_tc_merge_kernel(const MergeParams p) {
     int r = 0;
     float tau = INFINITY;
     unsigned long long unused = 0;
-    for (std::uint32_t ch = 0; ch < p.nchunks; ++ch) {
-        const std::size_t at = (static_cast<std::size_t>(row) * p.nchunks + ch) * p.kc;
+    for (std::uint32_t ch = 0; ch < p.lists; ++ch) {
+        const std::size_t at = (static_cast<std::size_t>(row) * p.lists + ch) * p.kc;
         for (std::uint32_t j0 = 0; j0 < p.kc; j0 += 32) {
-            // kc may be 16: lanes past this chunk's list read nothing.
+            // kc may be 16: lanes past this list's end read nothing.
             const bool in = j0 + lane < p.kc;
             const std::uint32_t id = in ? p.cand_ids[at + j0 + lane] : kNoId;
             const float d = in ? p.cand_d[at + j0 + lane] : INFINITY;
             merge_round(rd, rid, r, static_cast<int>(p.kc), d, id, id < p.n, ap, lane, unused);
         }
-        tau = fminf(tau, p.cand_tau[static_cast<std::size_t>(row) * p.nchunks + ch]);
+        tau = fminf(tau, p.cand_tau[static_cast<std::size_t>(row) * p.lists + ch]);
     }
     if (r == static_cast<int>(p.kc)) {
         tau = fminf(tau, rd[r - 1]);  // every candidate dropped here was at least this far
@@ -795,7 +880,7 @@ std::size_t align_up(std::size_t x, std::size_t a) { return (x + a - 1) / a * a;
 std::atomic<std::uint64_t> g_tc_wait_ns{kWaitNs};
 
 struct Plan {
-    std::uint32_t dk, kchunks, kc, stages, qtiles, nchunks, chunk_rows, halves;
+    std::uint32_t dk, kchunks, kc, stages, qtiles, nchunks, tpq, grid, halves;
     std::uint32_t off_b, off_lists, off_bar;
     std::size_t smem;
     bool ok;
@@ -838,11 +923,26 @@ Plan make_plan(std::uint32_t nq, std::uint32_t n, std::uint32_t dim, std::uint32
     pl.off_bar = static_cast<std::uint32_t>(pl.off_lists + lists);
     pl.smem = 1024 + pl.off_bar + 8 * (2 * stages) + 64 + 16;
     pl.qtiles = (nq + kBM - 1) / kBM;
-    // Chunks of the stored rows: about 8 work items per SM, at least one tile each.
-    const std::uint32_t target = std::max<std::uint32_t>(1, (8u * sms + pl.qtiles - 1) / pl.qtiles);
-    std::uint32_t rows = static_cast<std::uint32_t>(align_up((n + target - 1) / target, kBN));
-    pl.chunk_rows = std::max<std::uint32_t>(rows, kBN);
-    pl.nchunks = (n + pl.chunk_rows - 1) / pl.chunk_rows;
+    // Chunks of the stored rows: the fewest whose (query tile, chunk) items fill the waves of
+    // one CTA per SM to 97 % (the last wave's idle SMs are the loss), else the best filling.
+    pl.tpq = (n + kBN - 1) / kBN;
+    const std::uint32_t most = std::min<std::uint32_t>(pl.tpq, 2u * static_cast<std::uint32_t>(sms));
+    double best = 0.0;
+    pl.nchunks = 1;
+    for (std::uint32_t c = 1; c <= most; ++c) {
+        const std::uint64_t items = static_cast<std::uint64_t>(pl.qtiles) * c;
+        const std::uint64_t waves = (items + sms - 1) / sms;
+        const double fill = static_cast<double>(items) / static_cast<double>(waves * sms);
+        if (fill > best + 1e-9) {
+            best = fill;
+            pl.nchunks = c;
+        }
+        if (fill >= 0.97) {
+            break;
+        }
+    }
+    pl.grid = static_cast<std::uint32_t>(std::min<std::uint64_t>(
+        static_cast<std::uint64_t>(pl.qtiles) * pl.nchunks, static_cast<std::uint64_t>(sms)));
     return pl;
 }
 
@@ -1025,7 +1125,7 @@ cudaError_t launch_bruteforce_tc(const BruteArgs& a, const TcBase& b, void* work
     p.qtiles = pl.qtiles;
     p.nchunks = pl.nchunks;
     p.halves = pl.halves;
-    p.chunk_rows = pl.chunk_rows;
+    p.tpq = pl.tpq;
     p.kc = pl.kc;
     p.stages = pl.stages;
     p.metric = a.base.metric == 0 ? 0u : 1u;
@@ -1052,9 +1152,7 @@ cudaError_t launch_bruteforce_tc(const BruteArgs& a, const TcBase& b, void* work
     if (err != cudaSuccess) {
         return err;
     }
-    const std::uint32_t items = pl.qtiles * pl.nchunks;
-    const std::uint32_t grid = std::min<std::uint32_t>(items, static_cast<std::uint32_t>(sms));
-    bf_tc_kernel<<<grid, kThreads, pl.smem, stream>>>(mq_hi, mq_lo, b.map_hi, b.map_lo, p);
+    bf_tc_kernel<<<pl.grid, kThreads, pl.smem, stream>>>(mq_hi, mq_lo, b.map_hi, b.map_lo, p);
     if ((err = cudaGetLastError()) != cudaSuccess) {
         return err;
     }
@@ -1064,7 +1162,7 @@ cudaError_t launch_bruteforce_tc(const BruteArgs& a, const TcBase& b, void* work
     m.n = n;
     m.dim = dim;
     m.row32 = row32;
-    m.nchunks = static_cast<std::uint32_t>(lists);  // candidate lists per query
+    m.lists = static_cast<std::uint32_t>(lists);  // candidate lists per query
     m.kc = pl.kc;
     m.k = a.k;
     m.out_stride = a.out_stride;
