@@ -139,6 +139,55 @@ __device__ __forceinline__ void mma_commit(std::uint32_t mbar) {
         "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
         : "memory");
 }
+// The MMAs of one 128 x 128 tile: K in KC chunks of 64, 16 per MMA, the hi * hi products plus
+// hi * lo (XLO) and lo * hi (QLO) when the data need them. Fully unrolled with compile-time
+// offsets: issued from a loop with a run-time trip count and branches, each MMA took about three
+// times as long to issue as the tensor core takes to run it (measured on a B200).
+template <int KC, bool XLO, bool QLO>
+__device__ __forceinline__ void mma_tile(std::uint32_t d_tmem, std::uint32_t a_hi, std::uint32_t a_lo,
+                                         std::uint32_t bs) {
+#pragma unroll
+    for (int c = 0; c < KC; ++c) {
+#pragma unroll
+        for (int kk = 0; kk < kBK / 16; ++kk) {
+            const std::uint32_t off = static_cast<std::uint32_t>(c) * kChunk + static_cast<std::uint32_t>(kk) * 32;
+            const std::uint64_t ah = sw128_desc(a_hi + off);
+            const std::uint64_t bh = sw128_desc(bs + off);
+            mma_bf16(d_tmem, ah, bh, (c | kk) != 0 ? 1u : 0u);
+            if (XLO) {
+                mma_bf16(d_tmem, ah, sw128_desc(bs + KC * kChunk + off), 1u);
+            }
+            if (QLO) {
+                mma_bf16(d_tmem, sw128_desc(a_lo + off), bh, 1u);
+            }
+        }
+    }
+}
+template <int KC>
+__device__ __forceinline__ void mma_tile_terms(bool xlo, bool qlo, std::uint32_t d_tmem, std::uint32_t a_hi,
+                                               std::uint32_t a_lo, std::uint32_t bs) {
+    if (xlo) {
+        if (qlo) {
+            mma_tile<KC, true, true>(d_tmem, a_hi, a_lo, bs);
+        } else {
+            mma_tile<KC, true, false>(d_tmem, a_hi, a_lo, bs);
+        }
+    } else if (qlo) {
+        mma_tile<KC, false, true>(d_tmem, a_hi, a_lo, bs);
+    } else {
+        mma_tile<KC, false, false>(d_tmem, a_hi, a_lo, bs);
+    }
+}
+// One tile's MMAs for kchunks in 1..4 (the plan admits no other count).
+__device__ __forceinline__ void mma_tile_any(std::uint32_t kchunks, bool xlo, bool qlo, std::uint32_t d_tmem,
+                                             std::uint32_t a_hi, std::uint32_t a_lo, std::uint32_t bs) {
+    switch (kchunks) {
+        case 1: mma_tile_terms<1>(xlo, qlo, d_tmem, a_hi, a_lo, bs); break;
+        case 2: mma_tile_terms<2>(xlo, qlo, d_tmem, a_hi, a_lo, bs); break;
+        case 3: mma_tile_terms<3>(xlo, qlo, d_tmem, a_hi, a_lo, bs); break;
+        default: mma_tile_terms<4>(xlo, qlo, d_tmem, a_hi, a_lo, bs); break;
+    }
+}
 __device__ __forceinline__ void tmem_ld32(std::uint32_t taddr, std::uint32_t (&r)[32]) {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
@@ -402,22 +451,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                     break;
                 }
                 tc_fence_after();
-                const std::uint32_t d_tmem = tmem + b * kBN;
-                const std::uint32_t bs = b0 + s * stage_bytes;
-                for (std::uint32_t c = 0; c < p.kchunks; ++c) {
-                    for (std::uint32_t kk = 0; kk < kBK / 16; ++kk) {
-                        const std::uint32_t off = c * kChunk + kk * 32;
-                        const std::uint64_t ah = sw128_desc(a_hi + off);
-                        const std::uint64_t bh = sw128_desc(bs + off);
-                        mma_bf16(d_tmem, ah, bh, (c | kk) != 0 ? 1u : 0u);
-                        if (xlo) {
-                            mma_bf16(d_tmem, ah, sw128_desc(bs + p.kchunks * kChunk + off), 1u);
-                        }
-                        if (qlo) {
-                            mma_bf16(d_tmem, sw128_desc(a_lo + off), bh, 1u);
-                        }
-                    }
-                }
+                mma_tile_any(p.kchunks, xlo, qlo, tmem + b * kBN, a_hi, a_lo, b0 + s * stage_bytes);
                 mma_commit(empty(s));
                 mma_commit(tfull0 + 8 * b);
             }
