@@ -767,6 +767,7 @@ struct MergeParams {
     std::uint32_t* out_counts;
     std::uint32_t* uncertified;    // [nq] rows, count in uncertified_count
     std::uint32_t* uncertified_count;
+    const std::uint32_t* status;   // the call's status word (nonzero: the call has failed)
 };
 
 template <bool kL2>
@@ -783,7 +784,10 @@ __global__ void bf_tc_merge_kernel(const MergeParams p) {
     std::uint32_t* eid = reinterpret_cast<std::uint32_t*>(ws + p.row32 * 4 + p.kc * 12);
     int* ap = reinterpret_cast<int*>(ws + p.row32 * 4 + p.kc * 16);
     const std::uint32_t row = blockIdx.x * (blockDim.x >> 5) + warp;
-    if (row >= p.nq) {
+    // After a failed scoring pass (a timed-out wait) the candidate lists were never written:
+    // nothing here may read them (their stale contents are no valid merge input), and the call
+    // reports the failure.
+    if (row >= p.nq || *p.status != 0) {
         return;
     }
     std::uint32_t* oid = p.out_ids + static_cast<std::size_t>(row) * p.out_stride;
@@ -1217,6 +1221,7 @@ cudaError_t launch_bruteforce_tc(const BruteArgs& a, const TcBase& b, void* work
     m.out_counts = a.out_counts;
     m.uncertified = uncert;
     m.uncertified_count = uncertified_out;
+    m.status = a.status;
     // The stored vectors' largest norm, as the prep kernel left it in the base's flag words.
     m.xmax = reinterpret_cast<const float*>(static_cast<const std::uint32_t*>(b.flags) + 1);
     const int warps = 8;
