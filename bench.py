@@ -39,7 +39,9 @@ N_BASE = 1_000_000
 N_QUERIES = 10_000
 K = 10
 M, EF_CONSTRUCTION, SEED = 16, 200, 42
-EF_SWEEP = [16, 20, 24, 28, 32, 36, 40, 44, 48, 56, 64, 80, 96, 128, 192, 256, 384, 512]
+# Operating points: both arms walk this list upwards and stop at the first ef reaching the recall
+# target, so the list is dense (step 1) where that ef lies for this workload and coarse elsewhere.
+EF_SWEEP = [16, 20, 24] + list(range(28, 49)) + [56, 64, 80, 96, 128, 192, 256, 384, 512]
 # ef values of the id-parity comparison with the reference (the config-2 sweep, 16..512).
 PARITY_EFS = [16, 24, 32, 48, 64, 96, 128, 192, 256, 384, 512]
 PARITY_MIN_IDS = 0.999    # share of queries whose k ids equal the reference's, at every ef
