@@ -302,6 +302,7 @@ struct TcParams {
     float* cand_d;
     float* cand_tau;                      // [nq][nchunks * halves]
     std::uint32_t* floor_key;             // [nq] best kc-th score any list holds (ordered key)
+    std::uint32_t* quarter_key;           // [nq][nchunks * halves] each list's (kc / 4)-th score
     std::uint32_t* error;                 // status word: 5 on a timeout
     std::uint64_t wait_ns;                // limit of each pipeline wait (the drains keep kWaitNs)
     std::uint32_t off_b, off_lists, off_bar;  // smem offsets from the 1024-aligned base
@@ -585,8 +586,10 @@ __global__ void __launch_bounds__(kThreads, 1)
                     }
                 }
                 if (live && (t & 31u) == 31u) {
-                    // Every 32 tiles: publish this list's kc-th (its kc entries only improve)
-                    // and take up a better floor from the query's other lists.
+                    // Every 32 tiles: publish this list's kc-th and (kc / 4)-th scores (a list's
+                    // entries only improve, so both only rise) and take up a better floor from
+                    // the query's lists: the best kc-th, or the 4th highest of the (kc / 4)-th
+                    // scores (four lists then hold kc / 4 entries each at or above it).
                     std::uint32_t key;
                     if (count == p.kc) {
                         const std::uint32_t mine = float_to_key(list_d[(p.kc - 1) * kBM + e]);
@@ -594,6 +597,26 @@ __global__ void __launch_bounds__(kThreads, 1)
                     } else {
                         key = __ldcg(p.floor_key + row);
                     }
+                    const std::uint32_t quarter = p.kc >> 2;
+                    std::uint32_t* qk = p.quarter_key + static_cast<std::size_t>(row) * lists;
+                    if (count >= quarter) {
+                        __stcg(qk + ch * p.halves + half, float_to_key(list_d[(quarter - 1) * kBM + e]));
+                    }
+                    std::uint32_t k0 = 0, k1 = 0, k2 = 0, k3 = 0;  // the four highest, k0 >= .. >= k3
+                    for (std::uint32_t l = 0; l < lists; ++l) {
+                        std::uint32_t v = __ldcg(qk + l);
+                        std::uint32_t m = max(k0, v);
+                        v = min(k0, v);
+                        k0 = m;
+                        m = max(k1, v);
+                        v = min(k1, v);
+                        k1 = m;
+                        m = max(k2, v);
+                        v = min(k2, v);
+                        k2 = m;
+                        k3 = max(k3, v);
+                    }
+                    key = max(key, k3);
                     const float fl = key_to_float(key);
                     if (fl > floor) {
                         floor = fl;
@@ -625,6 +648,10 @@ __global__ void __launch_bounds__(kThreads, 1)
                     bound == -INFINITY ? INFINITY : (l2 ? __fsub_rn(qn, bound) : __fsub_rn(1.0F, bound));
                 if (count == p.kc) {
                     atomicMax(p.floor_key + row, float_to_key(list_d[(p.kc - 1) * kBM + e]));
+                }
+                if (count >= (p.kc >> 2)) {
+                    __stcg(p.quarter_key + static_cast<std::size_t>(row) * lists + ch * p.halves + half,
+                           float_to_key(list_d[((p.kc >> 2) - 1) * kBM + e]));
                 }
             }
         }
@@ -1082,7 +1109,7 @@ std::size_t bruteforce_tc_workspace(std::uint32_t nq, std::uint32_t n, std::uint
     return 4 * nqp * dk                         // q hi + lo
            + 4 * nqp * row32                    // normalized FP32 queries
            + 4 * nqp * 3                        // norms, exact and valid flags
-           + nq * chunks * kc * 8 + nq * chunks * 4  // candidates
+           + nq * chunks * kc * 8 + nq * chunks * 8  // candidates, bounds, quarter keys
            + 8 * nqp + 4096 + 16 * 256;         // uncertified rows, floors, flags, alignment
 }
 
@@ -1119,11 +1146,13 @@ cudaError_t launch_bruteforce_tc(const BruteArgs& a, const TcBase& b, void* work
     auto* cand_tau = reinterpret_cast<float*>(take(static_cast<std::size_t>(nq) * lists * 4));
     auto* uncert = reinterpret_cast<std::uint32_t*>(take(nqp * 4));
     auto* floor_key = reinterpret_cast<std::uint32_t*>(take(nqp * 4));
+    auto* quarter_key = reinterpret_cast<std::uint32_t*>(take(static_cast<std::size_t>(nq) * lists * 4));
     auto* flags = reinterpret_cast<std::uint32_t*>(take(64));  // [0] query flags [1] max norm [2] error
 
     cudaError_t err = cudaMemsetAsync(flags, 0, 64, stream);
     // Zero keys decode to -inf: no floor yet.
     if (err == cudaSuccess) err = cudaMemsetAsync(floor_key, 0, nqp * 4, stream);
+    if (err == cudaSuccess) err = cudaMemsetAsync(quarter_key, 0, static_cast<std::size_t>(nq) * lists * 4, stream);
     if (err == cudaSuccess) err = cudaMemsetAsync(uncertified_out, 0, 4, stream);
     if (err == cudaSuccess && nqp > nq) {
         err = cudaMemsetAsync(q_hi + static_cast<std::size_t>(nq) * pl.dk, 0, (nqp - nq) * pl.dk * 2, stream);
@@ -1175,6 +1204,7 @@ cudaError_t launch_bruteforce_tc(const BruteArgs& a, const TcBase& b, void* work
     p.cand_d = cand_d;
     p.cand_tau = cand_tau;
     p.floor_key = floor_key;
+    p.quarter_key = quarter_key;
     p.error = a.status;
     p.wait_ns = tc_wait_ns();
     p.off_b = pl.off_b;
