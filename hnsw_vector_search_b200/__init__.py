@@ -414,7 +414,10 @@ class BruteForceIndex:
         a = _rows(rows, self._dim)
         _raise(lib().vdx_bf_add(self._h, _ptr(a), a.shape[0], a.shape[1] if a.ndim == 2 else self._dim))
 
-    def search_batch(self, queries, k: int, method: str = "exact"):
+    def search_batch(self, queries, k: int, method: str = "tensor_core"):
+        """(ids, distances, counts) of the k closest stored vectors per query. "tensor_core" (the
+        default) returns the same ids and distance bits as "exact" (certified candidates from the
+        tensor cores, exact fallback per query); "exact" scores every pair on the CUDA cores."""
         q = _rows(queries, self._dim)
         nq = q.shape[0]
         kk = max(int(k), 0)
@@ -426,7 +429,7 @@ class BruteForceIndex:
                                          kk, m, _ptr(ids), _ptr(dists), _ptr(counts)))
         return ids, dists, counts
 
-    def search_batch_device(self, queries, k: int, ids, dists, counts, work, method="exact",
+    def search_batch_device(self, queries, k: int, ids, dists, counts, work, method="tensor_core",
                             stream=0) -> None:
         """Asynchronous device-buffer brute force (torch CUDA tensors)."""
         m = {"exact": 0, "tensor_core": 1}[method]

@@ -22,7 +22,9 @@ struct DeviceBase;
 // Which kernel scores the batch.
 enum class BruteMethod : std::uint8_t {
     Exact = 0,        // CUDA cores, every distance in the reference's FP32 order
-    TensorCore = 1,   // tcgen05 split-BF16 GEMM candidates, exact re-rank, certified
+    TensorCore = 1,   // tcgen05 split-BF16 GEMM candidates, exact re-rank, certified: the same
+                      // ids and distance bits as Exact (shapes it does not cover run Exact); the
+                      // default
 };
 
 class BruteForceIndex {
@@ -46,7 +48,7 @@ public:
     // search() for every row, one GPU batch, into caller buffers (padded like
     // HnswIndex::search_batch_into).
     void search_batch_into(MatrixView<float> queries, std::size_t k, Id* ids, float* distances,
-                           std::uint32_t* counts, BruteMethod method = BruteMethod::Exact,
+                           std::uint32_t* counts, BruteMethod method = BruteMethod::TensorCore,
                            int device = 0, const char* where = "BruteForceIndex::search") const;
 
     // The device-buffer form: queries, results and the work words (status, first failing row,
