@@ -115,6 +115,24 @@ def test_tensor_core_equals_exact_at_scale(gpu, metric, make):
         np.testing.assert_array_equal(a[1].view(np.uint32), b[1].view(np.uint32))
 
 
+@pytest.mark.parametrize("dim,nq", [(200, 1), (256, 129), (40, 3)])
+@pytest.mark.parametrize("k", [1, 24, 48])
+def test_tensor_core_equals_exact_across_shapes(gpu, dim, nq, k):
+    """The shapes the work split and the MMA sequence specialize on: 1 to 4 K chunks of 64 (d 40,
+    200, 256), a single query tile split into many short chunks (nq 1 or 3: each chunk a tile or
+    two), candidate lists of 16, 32 and 64 (k 1, 24, 48) with their quarter-rank floors, integer
+    data (exact scores) and real-valued data (lo terms, certification margins)."""
+    for base, queries in ((integer_matrix(9_000, dim, 21), integer_matrix(nq, dim, 22)),
+                          (uniform_matrix(9_000, dim, 23), uniform_matrix(nq, dim, 24))):
+        bf = gpu.BruteForceIndex(dim)
+        bf.add(base)
+        a = bf.search_batch(queries, k, method="exact")
+        b = bf.search_batch(queries, k, method="tensor_core")
+        np.testing.assert_array_equal(a[2], b[2])
+        np.testing.assert_array_equal(a[0], b[0])
+        np.testing.assert_array_equal(a[1].view(np.uint32), b[1].view(np.uint32))
+
+
 def test_tensor_core_matches_reference(gpu, orc):
     from hnsw_vector_search_b200 import datasets as ds
     base, queries = ds.config_sift_like(rows=20_000, n_queries=200)
