@@ -293,6 +293,20 @@ __device__ __forceinline__ void accumulate2(std::uint64_t& acc, std::uint64_t q,
     }
 }
 
+// acc += (x - q)^2 on two chains, x the two BF16 elements packed in w (element 2i in the low
+// half): sm_100's mixed-precision subtract takes the BF16 operand as it is (its conversion to
+// FP32 is exact) and rounds x - q once, like the FP32 subtract of the converted element, and
+// (x - q)^2 has the bits of (q - x)^2. One instruction per element instead of a conversion plus
+// half a paired subtract.
+__device__ __forceinline__ void accumulate2_l2_bf16(std::uint64_t& acc, std::uint32_t w, float q0,
+                                                    float q1) {
+    std::uint64_t d;
+    asm("{\n\t.reg .b16 lo, hi;\n\t.reg .f32 a, b;\n\tmov.b32 {lo, hi}, %1;\n\t"
+        "sub.rn.f32.bf16 a, lo, %2;\n\tsub.rn.f32.bf16 b, hi, %3;\n\tmov.b64 %0, {a, b};\n\t}"
+        : "=l"(d) : "r"(w), "f"(q0), "f"(q1));
+    asm("fma.rn.f32x2 %0, %1, %1, %2;" : "=l"(acc) : "l"(d), "l"(acc));
+}
+
 // The raw sum between the query and one row, computed by TWO lanes: `half` 0 runs the
 // reference's accumulator lanes 0..15 (elements 32t + 0..15), `half` 1 lanes 16..31 (elements
 // 32t + 16..31), two chains per paired instruction. Half 0 also runs the 8-element blocks
@@ -318,6 +332,16 @@ __device__ __forceinline__ float pair_raw(const float* q, const unsigned char* r
     const auto block32 = [&](std::uint32_t i) {
 #pragma unroll
         for (int u = 0; u < 16; u += E) {
+            if constexpr (P == kBF16 && kL2) {
+                const uint4 w = *reinterpret_cast<const uint4*>(row + 2 * (i + off + u));
+                const float4 qa = *reinterpret_cast<const float4*>(q + i + off + u);
+                const float4 qb = *reinterpret_cast<const float4*>(q + i + off + u + 4);
+                accumulate2_l2_bf16(acc[(u >> 1) + 0], w.x, qa.x, qa.y);
+                accumulate2_l2_bf16(acc[(u >> 1) + 1], w.y, qa.z, qa.w);
+                accumulate2_l2_bf16(acc[(u >> 1) + 2], w.z, qb.x, qb.y);
+                accumulate2_l2_bf16(acc[(u >> 1) + 3], w.w, qb.z, qb.w);
+                continue;
+            }
             float x[E];
             load16<P>(row, i + off + u, scale, x);
 #pragma unroll
