@@ -414,6 +414,70 @@ __device__ __forceinline__ float pair_distance(const float* q, const unsigned ch
     return kL2 ? raw : __fsub_rn(1.0F, raw);
 }
 
+// The raw sum between the query and one row of dimension kDim (a multiple of 32), computed by
+// FOUR lanes: quarter j runs the reference's accumulator lanes 8j..8j+7 (elements 32t + 8j..8j+7),
+// two chains per paired instruction, so each lane does a quarter of the row (a round of at most
+// 8 rows scores them in half the time of the two-lane form). The tree joins the quarters as
+// the reference adds (acc[l] + acc[l+8]) + (acc[l+16] + acc[l+24]): quarter 1 hands its sums to
+// quarter 0 and quarter 3 to quarter 2 (lane + 8), then quarter 2 to quarter 0 (lane + 16); the
+// horizontal tree follows. Call with row r's quarters in lanes r, r + 8, r + 16, r + 24, every
+// lane of the warp converged; the result is valid in quarter 0's lane. Same bits as pair_raw.
+// FP32 and BF16 rows only (a 16-byte FP8 load would straddle two quarters).
+template <int P, bool kL2, std::uint32_t kDim>
+__device__ __forceinline__ float quad_raw(const float* q, const unsigned char* row, int quarter) {
+    static_assert(kDim % 32 == 0 && kDim > 0, "quad_raw needs a dimension that is a multiple of 32");
+    static_assert(P != kFP8, "quad_raw reads 8 elements per lane and block");
+    std::uint64_t acc[4] = {0, 0, 0, 0};
+    const std::uint32_t off = 8u * static_cast<std::uint32_t>(quarter);
+#pragma unroll
+    for (std::uint32_t b = 0; b < kDim / 32; ++b) {
+        const std::uint32_t e = 32 * b + off;
+        const float4 qa = *reinterpret_cast<const float4*>(q + e);
+        const float4 qb = *reinterpret_cast<const float4*>(q + e + 4);
+        if constexpr (P == kBF16 && kL2) {
+            const uint4 w = *reinterpret_cast<const uint4*>(row + 2 * e);
+            accumulate2_l2_bf16(acc[0], w.x, qa.x, qa.y);
+            accumulate2_l2_bf16(acc[1], w.y, qa.z, qa.w);
+            accumulate2_l2_bf16(acc[2], w.z, qb.x, qb.y);
+            accumulate2_l2_bf16(acc[3], w.w, qb.z, qb.w);
+        } else {
+            float x[8];
+            if constexpr (P == kBF16) {
+                load16<P>(row, e, 1.0F, x);
+            } else {
+                load16<P>(row, e, 1.0F, x);
+                load16<P>(row, e + 4, 1.0F, x + 4);
+            }
+            accumulate2<kL2>(acc[0], pack2(qa.x, qa.y), pack2(x[0], x[1]));
+            accumulate2<kL2>(acc[1], pack2(qa.z, qa.w), pack2(x[2], x[3]));
+            accumulate2<kL2>(acc[2], pack2(qb.x, qb.y), pack2(x[4], x[5]));
+            accumulate2<kL2>(acc[3], pack2(qb.z, qb.w), pack2(x[6], x[7]));
+        }
+    }
+    float a[8];
+#pragma unroll
+    for (int l = 0; l < 4; ++l) {
+        unpack2(acc[l], a[2 * l], a[2 * l + 1]);
+    }
+#pragma unroll
+    for (int l = 0; l < 8; ++l) {
+        a[l] = __fadd_rn(a[l], __shfl_down_sync(kFull, a[l], 8));
+    }
+    float h[8];
+#pragma unroll
+    for (int l = 0; l < 8; ++l) {
+        h[l] = __fadd_rn(a[l], __shfl_down_sync(kFull, a[l], 16));
+    }
+    return __fadd_rn(__fadd_rn(__fadd_rn(h[0], h[4]), __fadd_rn(h[2], h[6])),
+                     __fadd_rn(__fadd_rn(h[1], h[5]), __fadd_rn(h[3], h[7])));
+}
+
+template <int P, bool kL2, std::uint32_t kDim>
+__device__ __forceinline__ float quad_distance(const float* q, const unsigned char* row, int quarter) {
+    const float raw = quad_raw<P, kL2, kDim>(q, row, quarter);
+    return kL2 ? raw : __fsub_rn(1.0F, raw);
+}
+
 // A shared-memory row stride for `row_bytes` rows read one row per lane with 16-byte loads:
 // an odd number of 16-byte units, so the 8 lanes of each load phase hit distinct banks.
 __host__ __device__ __forceinline__ std::uint32_t padded_row_stride(std::uint32_t row_bytes) {

@@ -239,6 +239,25 @@ __device__ __forceinline__ float row_distance(const float* q, const unsigned cha
                       : pair_distance<P, kL2>(q, row, dim, row_bytes, half);
 }
 
+// The distances of a round of `cnt` staged rows (warp-uniform), valid in lane r for row r: at
+// dimension 128 a round of at most 8 FP32 / BF16 rows is scored by four lanes a row
+// (quad_distance, row lane & 7), every other round by two (row_distance, row lane & 15). Same
+// bits either way. Rows past the round re-read the buffer's last row (results masked).
+template <int P, bool kL2>
+__device__ __forceinline__ float round_distance(const float* q, const unsigned char* rows,
+                                                std::uint32_t stride, const unsigned char* my_row,
+                                                std::uint32_t dim, std::uint32_t row_bytes, int half,
+                                                int lane, int cnt, int rows_cap) {
+    if constexpr (P != kFP8) {
+        if (dim == 128 && cnt <= 8) {
+            const int row = min(lane & 7, rows_cap - 1);
+            return quad_distance<P, kL2, 128>(q, rows + static_cast<std::uint32_t>(row) * stride,
+                                              lane >> 3);
+        }
+    }
+    return row_distance<P, kL2>(q, my_row, dim, row_bytes, half);
+}
+
 // Which learned-termination code a search kernel carries: none (plain searches), the stop only,
 // or the stop and the training traces.
 enum LearnMode : int { kLearnNone = 0, kLearnStop = 1, kLearnTrace = 2 };
@@ -466,7 +485,8 @@ __global__ void __launch_bounds__(kMaxThreads<P, kRegR>,
                             lane < cnt ? (compact ? fresh_ua[s0 + lane] : g.upper_at[fresh[s0 + lane]]) : 0u;
                         cp_async_wait<0>();
                         __syncwarp();
-                        const float pd = row_distance<P, kL2>(q, my_row, g.dim, g.row_bytes, half);
+                        const float pd = round_distance<P, kL2>(q, rows, stride_s, my_row, g.dim,
+                                                                g.row_bytes, half, lane, cnt, rounds_cap);
                         float d = INFINITY;
                         int idx = 0x7FFFFFFF;
                         if (lane < cnt) {
@@ -683,7 +703,8 @@ __global__ void __launch_bounds__(kMaxThreads<P, kRegR>,
                 }
                 __syncwarp();
                 const bool valid = lane < cnt;
-                const float pd = row_distance<P, kL2>(q, my_row, g.dim, g.row_bytes, half);
+                const float pd = round_distance<P, kL2>(q, rows, stride_s, my_row, g.dim, g.row_bytes,
+                                                        half, lane, cnt, rounds_cap);
                 const float my_d = valid ? pd : INFINITY;
                 const std::uint32_t my_id = valid ? fresh[s0 + lane] : kNoId;
                 c_d0 += cnt;

@@ -77,7 +77,7 @@ def test_gpu_counters_equal_the_oracles(gpu, orc, small_l2):
 
 
 @pytest.mark.parametrize("metric", [0, 1, 2])
-@pytest.mark.parametrize("dim", [16, 13, 100, 40])
+@pytest.mark.parametrize("dim", [16, 13, 100, 40, 128])
 def test_gpu_equals_reference_on_real_valued_data(gpu, orc, tmp_path, metric, dim):
     base = uniform_matrix(1500, dim, 1)
     queries = uniform_matrix(80, dim, 2)
@@ -276,14 +276,15 @@ def _exact(orc, metric, q, row):
 
 @pytest.mark.parametrize("precision", ["bf16", "fp8"])
 @pytest.mark.parametrize("metric", [0, 1, 2])
-def test_low_precision_traversal_equals_the_quantized_oracle(gpu, orc, tmp_path, precision, metric):
+@pytest.mark.parametrize("dim", [40, 128])
+def test_low_precision_traversal_equals_the_quantized_oracle(gpu, orc, tmp_path, precision, metric, dim):
     """BF16 / FP8 traversal on real-valued data, bit for bit. The oracle quantizes the stored
     rows as the GPU does (round to nearest even; E4M3 with the per-row FP32 scale max|x| / 448)
     and runs the reference's search on them: with rerank="none" the GPU returns exactly those ids
     and distances. With a re-rank of r, the GPU's result is the oracle's best min(r, ef)
     candidates re-scored with the exact FP32 distance in the reference's order, best k by
-    (distance, id)."""
-    dim = 40
+    (distance, id). Dimension 128 runs the kernels' unrolled distance routines (two lanes a row,
+    and four lanes a row in rounds of at most 8 rows); real-valued data checks their order."""
     base = uniform_matrix(2000, dim, 11)
     queries = uniform_matrix(120, dim, 12)
     ref = orc.RefHnsw(dim, metric, 8, 60, 42)
