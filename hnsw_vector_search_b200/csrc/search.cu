@@ -275,6 +275,16 @@ __global__ void __launch_bounds__(kMaxThreads<P, kRegR>,
                                   kLowRegs<P, kRegR> ? 5 : (kLearn != kLearnNone ? 0 : 2))
     search_kernel(const SearchArgs a) {
     constexpr std::uint32_t pass = kPass;
+    // Ordered launch: order_kernel and the layer-0 pass are launched as programmatic dependents
+    // (they may start while the kernel before them finishes); the descent lets its dependent
+    // launch at once, and the layer-0 pass waits in hardware until order_kernel has completed
+    // and its writes are visible. Without that launch attribute the wait returns at once.
+    if constexpr (kPass == 1) {
+        asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    }
+    if constexpr (kPass == 2) {
+        asm volatile("griddepcontrol.wait;" ::: "memory");
+    }
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = static_cast<int>(threadIdx.x & 31);
     const int warp = static_cast<int>(threadIdx.x >> 5);
@@ -970,6 +980,10 @@ __device__ __forceinline__ std::uint32_t order_bucket(const SearchArgs& a, std::
 }
 
 __global__ void __launch_bounds__(kOrderThreads) order_kernel(const SearchArgs a) {
+    // A programmatic dependent of the descent pass: the layer-0 pass may launch now; this kernel
+    // waits in hardware until the descent has completed and its entries are visible.
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     __shared__ std::uint32_t count[kOrderBuckets];
     __shared__ std::uint32_t warp_sum[kOrderThreads / 32];
     const std::uint32_t nq = a.nq_device != nullptr ? min(*a.nq_device, a.nq) : a.nq;
@@ -1190,18 +1204,34 @@ cudaError_t launch_typed(SearchArgs& args, const SearchPlan& plan, std::size_t s
     if (err = check_tables(blocks2); err != cudaSuccess) {
         return err;
     }
+    // order_kernel and the layer-0 pass as programmatic dependents of the kernel before each
+    // (their launch overlaps its end; griddepcontrol.wait in each orders the memory).
+    const auto launch_dependent = [&](const void* kernel, int blocks, int block_threads,
+                                      std::size_t shared) -> cudaError_t {
+        cudaLaunchAttribute attr[1] = {};
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(static_cast<unsigned>(blocks));
+        cfg.blockDim = dim3(static_cast<unsigned>(block_threads));
+        cfg.dynamicSmemBytes = shared;
+        cfg.stream = stream;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        void* params[] = {&args};
+        return cudaLaunchKernelExC(&cfg, kernel, params);
+    };
     args.pass = 1;
     if (err = launch_walk(k1, blocks1); err != cudaSuccess) {
         return err;
     }
-    order_kernel<<<1, kOrderThreads, 0, stream>>>(args);
-    if (err = cudaGetLastError(); err != cudaSuccess) {
+    if (err = launch_dependent(reinterpret_cast<const void*>(&order_kernel), 1, kOrderThreads, 0);
+        err != cudaSuccess) {
         return err;
     }
     args.pass = 2;
-    reinterpret_cast<Kernel>(const_cast<void*>(k2))<<<blocks2, threads, smem, stream>>>(args);
     g_last_kernels = 3;
-    return cudaGetLastError();
+    return launch_dependent(k2, blocks2, threads, smem);
 }
 
 }  // namespace
